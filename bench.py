@@ -1,0 +1,380 @@
+"""Benchmark of the batched tridiagonal solve on B200.
+
+Workload (one step): the 512^3 FP64 grid solved along x, then y, then z with
+tridDmtsvStridedBatch, d overwritten by each solve (the order of the ADI
+heat solver, apps/adi/src/adi_cuda.cu:294-323); 3 * 512^3 elements per step.
+Inputs are seeded synthetic data with the distribution the configs name
+(a, c ~ U(-0.5, 0.5), b = 1 + |a| + |c| + U(0, 1), d ~ N(0, 1)); every array
+(1 GiB) is larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`value` is device throughput with inputs resident in HBM; `e2e` is the same
+metric through the C ABI with host arrays (pinned host -> device copies of
+a, b, c, d and the device -> host copy of the result inside the timed
+region). `cpu_baseline` times the reference's own CPU library (oracle/_ref)
+on the host cores on a bounded slab of the same workload. With --impl
+reference only that CPU timing runs, as the reference arm.
+
+Multi-GPU: one process per GPU (torchrun); the solve shards by systems with
+no exchange, so every rank solves its own grid (weak scaling) and value is
+the sum over ranks / the max over ranks of the timed region.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+# The reference CPU library keeps 2*N_MAX SIMD vectors on each OpenMP
+# worker's stack; set before any OpenMP runtime starts.
+os.environ.setdefault("OMP_STACKSIZE", "32M")
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "elements/s & HBM GB/s (x/y/z, 512^3 FP64); FP32+refine vs FP64 at 1e-12"
+UNIT = "elements/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-planes", type=int, default=32,
+                    help="slab thickness of the CPU sample (planes of n*n)")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="0 = as many as fit in ~10 s")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, STREAM-style copy)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback (6.65 TB/s pool measurement)"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and not line.startswith("#"):
+                    out[parts[0]] = float(parts[1])
+    except OSError:
+        pass
+    return out
+
+
+# ---- clocks -----------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        # samples under load: the upper half of the clock distribution is not a
+        # selection here; report the median of all samples taken in the region
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- CPU reference timing ---------------------------------------------------------
+
+def cpu_reference_rate(n, planes, steps, dtype, time_budget=10.0):
+    """elements/s of the reference CPU library (oracle/_ref) on a slab sample:
+    x and y solves on n*n*planes, the z solve on n*planes*n (every system keeps
+    its full length n). Returns (rate, info dict)."""
+    import numpy as np
+
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+
+    ref = Reference()
+    npdt = np.float64 if dtype == "f64" else np.float32
+    m = n * n * planes
+    rng = np.random.default_rng(1)
+    a = rng.uniform(-0.5, 0.5, m).astype(npdt)
+    c = rng.uniform(-0.5, 0.5, m).astype(npdt)
+    b = (1 + np.abs(a) + np.abs(c) + rng.uniform(0, 1, m)).astype(npdt)
+    d = rng.standard_normal(m).astype(npdt)
+    plan = [([n, n, planes], 0), ([n, n, planes], 1), ([n, planes, n], 2)]
+
+    def step():
+        for dims, sd in plan:
+            ref.strided_batch(a, b, c, d, dims, sd)
+
+    step()  # warm-up (page faults, thread start)
+    t0 = time.perf_counter()
+    step()
+    one = time.perf_counter() - t0
+    if steps <= 0:
+        steps = max(2, min(50, int(time_budget / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    el = time.perf_counter() - t0
+    rate = 3 * m * steps / el
+    info = {"cores": threads, "kind": "reference",
+            "sample": f"{steps} steps of x,y solves on {n}x{n}x{planes} and the z solve on "
+                      f"{n}x{planes}x{n} ({dtype}, reference scalar/src/cpu/trid_cpu.cpp "
+                      f"built -O3 -fopenmp, {ref.isa}), {el:.2f} s",
+            "lib": os.path.basename(ref.path)}
+    return rate, info
+
+
+# ---- the GPU arm ------------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import tridsolver_b200 as tb
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    n = args.n
+    shape = (n, n, n)
+    dims = [n, n, n]
+    tdt = torch.float64 if args.dtype == "f64" else torch.float32
+    es = 8 if args.dtype == "f64" else 4
+    g = torch.Generator(device=dev).manual_seed(1234 + rank)
+    a = torch.rand(shape, generator=g, device=dev, dtype=tdt) - 0.5
+    c = torch.rand(shape, generator=g, device=dev, dtype=tdt) - 0.5
+    b = 1 + a.abs() + c.abs() + torch.rand(shape, generator=g, device=dev, dtype=tdt)
+    d = torch.randn(shape, generator=g, device=dev, dtype=tdt)
+    solve = tb.tridDmtsvStridedBatch if args.dtype == "f64" else tb.tridSmtsvStridedBatch
+    elems = n ** 3
+
+    stream = torch.cuda.current_stream()
+    tb.set_stream(stream)
+    tb.set_blocking(False)
+
+    def step(evs=None):
+        for axis in range(3):
+            if evs is not None:
+                evs[axis][0].record(stream)
+            st = solve(None, a, b, c, d, 3, axis, dims, dims)
+            if st != 0:
+                raise RuntimeError(f"solve status {st}")
+            if evs is not None:
+                evs[axis][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    K = args.steps
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
+           for _ in range(K)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    gpu_index = vis.split(",")[local_rank] if vis else str(local_rank)
+    launches0 = tb.launch_count()
+    with ClockSampler(gpu_index) as clk:
+        torch.cuda.synchronize()
+        t_start.record(stream)
+        for k in range(K):
+            step(evs[k])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    launches = tb.launch_count() - launches0
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    axis_ms = [statistics.mean(evs[k][ax][0].elapsed_time(evs[k][ax][1]) for k in range(K))
+               for ax in range(3)]
+    vals = torch.tensor([total_ms] + axis_ms, dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
+    total_ms, axis_ms = vals[0].item(), [v.item() for v in vals[1:]]
+    ms_per_step = total_ms / K
+    value = world * 3 * elems * K / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host arrays (blocking calls)
+    e2e = None
+    if not args.no_e2e:
+        host = [t.cpu().pin_memory() for t in (a, b, c, d)]
+        out = torch.empty_like(host[3]).pin_memory()
+        tb.set_blocking(True)
+
+        def e2e_step():
+            for t, h in zip((a, b, c, d), host):
+                t.copy_(h, non_blocking=True)
+            for axis in range(3):
+                st = solve(None, a, b, c, d, 3, axis, dims, dims)
+                if st != 0:
+                    raise RuntimeError(f"solve status {st}")
+            out.copy_(d, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(ems, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": world * 3 * elems * args.e2e_steps / (ems.item() / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 4 * elems * es, "d2h_bytes_per_step": elems * es,
+               "ms_per_step": ems.item() / args.e2e_steps,
+               "path": "pinned host -> device copies of a,b,c,d, three blocking "
+                       "tridDmtsvStridedBatch calls, device -> host copy of d"}
+        tb.set_blocking(False)
+
+    hbm, hbm_src = peaks()
+    traffic = ncu_traffic()
+    names = ["x", "y", "z"]
+    alg_bytes = 5 * es * elems  # read a, b, c, d; write d
+    per_axis = {}
+    for ax in range(3):
+        gbs = alg_bytes / (axis_ms[ax] / 1e3) / 1e9
+        per_axis[names[ax]] = {
+            "ms": round(axis_ms[ax], 4),
+            "elements_per_s": elems / (axis_ms[ax] / 1e3),
+            "hbm_gbs": round(gbs, 1),
+            "frac_of_measured_peak": round(gbs / hbm, 4),
+            "plan": tb.describe_plan(es, dims, ax),
+        }
+    dom = max(range(3), key=lambda i: axis_ms[i])
+    dom_gbs = alg_bytes / (axis_ms[dom] / 1e3) / 1e9
+    key = f"{args.dtype}_n{n}_{names[dom]}"
+    roofline = {"bound": "hbm", "achieved": round(dom_gbs, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(dom_gbs / hbm, 4),
+                "traffic": traffic.get(key),
+                "kernel": f"solve along {names[dom]} ({per_axis[names[dom]]['plan']})",
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_source": hbm_src}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": f"{n}^3 {args.dtype.upper()} tridDmtsvStridedBatch along x, y, z "
+                                   f"(one step = 3 solves of {n * n} systems of length {n}, d "
+                                   "overwritten, ADI order)",
+                       "grid": dims, "parallelism": f"replicas x{world} (systems sharded by rank)",
+                       "l2": "inputs larger than L2 (each array "
+                             f"{elems * es / 2**30:.2f} GiB); no flush"},
+            "per_axis": per_axis, "roofline": roofline, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary()}
+    return line
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        planes = args.cpu_planes
+        rate, info = cpu_reference_rate(args.n, planes, args.steps, args.dtype)
+        line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": f"{args.n}^3 {args.dtype.upper()} solves along x, y, z, "
+                                       "sampled as slabs that keep every system's full length",
+                           "grid": [args.n] * 3},
+                "cpu_baseline": dict(info, value=rate, unit=UNIT),
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, info = cpu_reference_rate(args.n, args.cpu_planes, args.cpu_steps, args.dtype)
+        line["cpu_baseline"] = dict(info, value=rate, unit=UNIT)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,57 @@
+/*
+ * tridsolver_b200 — extensions beyond the reference's C ABI.
+ *
+ * Everything here is additive: the four reference entry points in
+ * tridsolver.h keep their exact signatures and semantics. These functions
+ * have no counterpart in scalar/include/tridsolver.h unless a line says so.
+ */
+#ifndef TRIDSOLVER_B200_H__
+#define TRIDSOLVER_B200_H__
+
+#include <stdint.h>
+
+#include "tridsolver.h"
+
+/* ---- execution control (per calling thread) ------------------------------
+ * The reference runs every solve on the legacy default stream and ends each
+ * call with cudaDeviceSynchronize (scalar/src/cuda/trid_cuda.cu:409-410).
+ * Here a call runs on the calling thread's stream (default: the legacy
+ * default stream, NULL) and, while blocking is on (the default), returns
+ * after a cudaStreamSynchronize of that stream. With blocking off, calls only
+ * enqueue work, so they can be captured into a CUDA graph. */
+EXTERN_C tridStatus_t tridSetStream(void *cuda_stream); /* a cudaStream_t */
+EXTERN_C void *tridGetStream(void);
+EXTERN_C tridStatus_t tridSetBlocking(int blocking);
+EXTERN_C int tridGetBlocking(void);
+
+/* Zero / non-finite pivots seen on the current device since the last call
+ * of this function (blocking calls also report them in their own status):
+ * TRID_STATUS_ZERO_PIVOT or TRID_STATUS_SUCCESS. Clears the record. */
+EXTERN_C tridStatus_t tridGetPivotStatus(void);
+
+/* Number of kernels this library has launched in this process. */
+EXTERN_C unsigned long long tridGetLaunchCount(void);
+
+/* ---- plan selection ------------------------------------------------------
+ * Kernel families, chosen per system length by the built-in table or the
+ * autotuner:
+ *   TRID_FAMILY_HYBRID  partition hybrid: T threads per system, M rows per
+ *                       thread, warp-shuffle PCR on the reduced system
+ *                       (T = 1 is thread-per-system Thomas);
+ *   TRID_FAMILY_PCR     pure PCR, one row per thread (systems <= 32 rows);
+ *   TRID_FAMILY_LONG    multi-block partition for long systems: reduced
+ *                       rows to scratch, recursive reduced solve, substitution.
+ * tridForcePlan(family, M) pins the choice for the calling thread (testing and
+ * tuning); family < 0 restores automatic selection. */
+#define TRID_FAMILY_AUTO (-1)
+#define TRID_FAMILY_HYBRID 0
+#define TRID_FAMILY_PCR 1
+#define TRID_FAMILY_LONG 2
+EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
+
+/* Describes the plan the next solve of this shape would use, e.g.
+ * "hybrid M=16 T=32 W=1 vec" (for logs and tests). Returns the length. */
+EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                              const int *pads, char *buf, int buflen);
+
+#endif

@@ -1,0 +1,104 @@
+"""CPU: the C-ABI library loads, exports every declared symbol and rejects bad
+arguments before touching a device (no compute calls here)."""
+
+import ctypes
+import subprocess
+
+import pytest
+
+import tridsolver_b200 as tb
+from tridsolver_b200 import _lib
+from tridsolver_b200.api import TridParams, TridStatus
+
+
+def test_library_loads():
+    lib = _lib.load()
+    assert lib is not None
+
+
+def test_exports_every_header_symbol():
+    declared = _lib.header_symbols()
+    # the reference's four entry points are among them
+    for name in ("tridDmtsvStridedBatch", "tridSmtsvStridedBatch", "tridDmtsvStridedBatchInc",
+                 "tridSmtsvStridedBatchInc"):
+        assert name in declared
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = [n for n in declared if n not in exported]
+    assert not missing, missing
+
+
+def test_tridparams_layout_matches_reference():
+    # struct TridParams {void *mpi_params; int opts[MAXDIM]; int sync;}
+    assert ctypes.sizeof(TridParams) == 24
+    assert TridParams.opts.offset == 8 and TridParams.sync.offset == 20
+
+
+BAD = [
+    dict(ndim=0, solvedim=0, dims=[4], pads=[4]),
+    dict(ndim=4, solvedim=0, dims=[4, 4, 4, 4], pads=[4, 4, 4, 4]),
+    dict(ndim=2, solvedim=2, dims=[4, 4], pads=[4, 4]),
+    dict(ndim=2, solvedim=-1, dims=[4, 4], pads=[4, 4]),
+    dict(ndim=2, solvedim=0, dims=[4, 4], pads=[3, 4]),     # pads[0] < dims[0]
+    dict(ndim=3, solvedim=1, dims=[4, 4, 4], pads=[4, 2, 4]),
+    dict(ndim=2, solvedim=0, dims=[-1, 4], pads=[4, 4]),
+]
+
+
+@pytest.mark.parametrize("case", BAD)
+@pytest.mark.parametrize("fn", ["tridDmtsvStridedBatch", "tridSmtsvStridedBatch"])
+def test_invalid_arguments(fn, case):
+    dummy = 4096  # never dereferenced: validation fails first
+    st = getattr(tb, fn)(None, dummy, dummy, dummy, dummy, case["ndim"], case["solvedim"],
+                         case["dims"], case["pads"])
+    assert st == TridStatus.INVALID_VALUE
+
+
+def test_null_pointer_rejected():
+    st = tb.tridDmtsvStridedBatch(None, None, 4096, 4096, 4096, 1, 0, [8], [8])
+    assert st == TridStatus.INVALID_VALUE
+    st = tb.tridDmtsvStridedBatchInc(None, 4096, 4096, 4096, 4096, None, 1, 0, [8], [8])
+    assert st == TridStatus.INVALID_VALUE
+
+
+def test_empty_problem_is_success_without_device():
+    st = tb.tridDmtsvStridedBatch(None, None, None, None, None, 2, 1, [0, 5], [0, 5])
+    assert st == TridStatus.SUCCESS
+    ctx = TridParams()
+    ctx.opts[0] = 4
+    st = tb.tridSmtsvStridedBatchInc(ctx, None, None, None, None, None, 3, 2, [3, 0, 2], [3, 1, 2])
+    assert st == TridStatus.SUCCESS
+
+
+@pytest.mark.parametrize("dtype_bytes,dims,solvedim,expect", [
+    (8, [512, 512, 512], 0, "hybrid M=16 T=32"),
+    (8, [512, 512, 512], 2, "hybrid M=16 T=32"),
+    (8, [256, 256, 256], 1, "hybrid M=8 T=32"),
+    (4, [1024, 8], 0, "hybrid M=32 T=32"),
+    (8, [100000], 0, "long"),
+    (8, [5, 7], 1, "hybrid M=8 T=1"),
+])
+def test_plan_table(dtype_bytes, dims, solvedim, expect):
+    assert tb.describe_plan(dtype_bytes, dims, solvedim).startswith(expect)
+
+
+def test_force_plan_round_trip():
+    tb.force_plan(tb.FAMILY_PCR)
+    assert tb.describe_plan(8, [20, 10], 0).startswith("pcr M=1 T=32")
+    tb.force_plan(tb.FAMILY_LONG, 8)
+    assert tb.describe_plan(8, [20, 10], 0).startswith("long M=8")
+    tb.force_plan(tb.FAMILY_HYBRID, 4)
+    assert tb.describe_plan(8, [20, 10], 0).startswith("hybrid M=4 T=8")
+    tb.force_plan()
+    with pytest.raises(tb.TridError):
+        tb.force_plan(tb.FAMILY_HYBRID, 3)
+
+
+def test_blocking_and_stream_settings():
+    assert tb.get_blocking() is True
+    tb.set_blocking(False)
+    assert tb.get_blocking() is False
+    tb.set_blocking(True)
+    tb.set_stream(None)
+    assert _lib.load().tridGetStream() in (None, 0)

@@ -1,0 +1,144 @@
+"""CPU: pin the oracle before trusting it.
+
+The plain-C restatement (oracle/trid_oracle.c) and the reference's own CPU
+library compiled from its sources (oracle/_ref) must both reproduce the golden
+fixtures made by the reference's generator, with the reference tests'
+tolerances and padded layouts (scalar/test/test_cpu.cpp:68-128, 175-352), and
+must agree with each other on seeded batches of every layout, odd sizes and
+the Inc variant.
+"""
+
+import numpy as np
+import pytest
+
+from fixtures import CASE_NAMES, allclose_ref, load_case
+from helpers import from_padded, make_system, normwise, pad_offset, to_padded
+from oracle.pyoracle import Reference, Restatement
+
+DTYPES = [np.float64, np.float32]
+
+
+@pytest.fixture(scope="module")
+def restatement():
+    return Restatement()
+
+
+@pytest.fixture(scope="module")
+def reference():
+    try:
+        return Reference()
+    except FileNotFoundError as e:  # the reference tree is not here
+        pytest.skip(str(e))
+
+
+def _expected(case, dt):
+    return case["u"] if dt == np.float64 else case["u_float"]
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("which", ["restatement", "reference"])
+def test_golden(which, name, dt, request):
+    lib = request.getfixturevalue(which)
+    case = load_case(name)
+    a, b, c, d = (np.ascontiguousarray(case[k].astype(dt)) for k in "abcd")
+    lib.strided_batch(a, b, c, d, case["dims"], case["solvedim"])
+    ok, worst, diff = allclose_ref(_expected(case, dt), d, dt)
+    assert ok, f"{which} {name} worst index {worst} diff {diff}"
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("which", ["restatement", "reference"])
+def test_golden_padded(which, name, dt, request):
+    """Every dimension padded by 2, pointers offset to the first interior
+    element (scalar/test/test_cpu.cpp:86-128)."""
+    lib = request.getfixturevalue(which)
+    case = load_case(name)
+    dims = case["dims"]
+    pads = [n + 2 for n in dims]
+    arrs = [to_padded(case[k].astype(dt), dims, pads, fill=0.0) for k in "abcd"]
+    off = pad_offset(pads)
+    views = [v[off:] for v in arrs]
+    lib.strided_batch(*views, dims, case["solvedim"], pads=pads)
+    out = from_padded(arrs[3], dims, pads)
+    ok, worst, diff = allclose_ref(_expected(case, dt), out, dt)
+    assert ok, f"{which} {name} worst index {worst} diff {diff}"
+    # padding untouched
+    mask = np.ones(arrs[3].size, bool)
+    from helpers import padded_index
+    mask[padded_index(dims, pads)] = False
+    assert np.all(arrs[3][mask] == 0.0)
+
+
+SHAPES = [([1], 0), ([7], 0), ([33, 5], 0), ([33, 5], 1), ([9, 10, 11], 0), ([9, 10, 11], 1),
+          ([9, 10, 11], 2), ([64, 64, 64], 0), ([64, 64, 64], 1), ([64, 64, 64], 2),
+          ([3, 1000], 1), ([1000, 2], 0)]
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("dims,solvedim", SHAPES)
+def test_restatement_matches_reference(dims, solvedim, inc, dt, restatement, reference):
+    a, b, c, d = make_system(dims, solvedim, dt, seed=len(dims) * 7 + solvedim)
+    u0 = np.random.default_rng(3).standard_normal(d.size).astype(dt) if inc else None
+    outs = []
+    for lib in (restatement, reference):
+        dd = d.copy()
+        uu = u0.copy() if inc else None
+        lib.strided_batch(a, b, c, dd, dims, solvedim, u=uu)
+        outs.append(uu if inc else dd)
+        if inc:
+            assert np.array_equal(dd, d), "Inc must leave d untouched"
+    tol = 1e-13 if dt == np.float64 else 2e-6
+    assert normwise(outs[0], outs[1]) <= tol
+
+
+def test_ragged_oracle_matches_reference_scalar(restatement, reference):
+    rng = np.random.default_rng(11)
+    lens = rng.integers(1, 300, size=40)
+    offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    n = int(offs[-1])
+    a, b, c, d = make_system([n], 0, np.float64, seed=5)
+    d1 = d.copy()
+    restatement.ragged(a, b, c, d1, offs)
+    d2 = d.copy()
+    for k in range(len(lens)):
+        s, e = offs[k], offs[k + 1]
+        seg = [np.ascontiguousarray(v[s:e]) for v in (a, b, c)]
+        dd = np.ascontiguousarray(d2[s:e])
+        reference.scalar(*seg, dd, e - s)
+        d2[s:e] = dd
+    assert normwise(d1, d2) <= 1e-13
+
+
+def test_adjoint_oracle_against_finite_differences(restatement):
+    dims, sd = [6, 20, 5], 1
+    a, b, c, d = make_system(dims, sd, np.float64, seed=21)
+    w = np.random.default_rng(2).standard_normal(d.size)
+    x = d.copy()
+    restatement.strided_batch(a, b, c, x, dims, sd)
+    abar, bbar, cbar, dbar = restatement.adjoint(a, b, c, x, w, dims, sd)
+
+    def loss(aa, bb, cc, dd):
+        xx = dd.copy()
+        restatement.strided_batch(aa, bb, cc, xx, dims, sd)
+        return float(np.dot(w, xx))
+
+    rng = np.random.default_rng(4)
+    h = 1e-6
+    for which, grad in (("a", abar), ("b", bbar), ("c", cbar), ("d", dbar)):
+        for idx in rng.integers(0, d.size, 20):
+            arrs = {"a": a, "b": b, "c": c, "d": d}
+            p = {k: v.copy() for k, v in arrs.items()}
+            m = {k: v.copy() for k, v in arrs.items()}
+            p[which][idx] += h
+            m[which][idx] -= h
+            fd = (loss(p["a"], p["b"], p["c"], p["d"]) - loss(m["a"], m["b"], m["c"], m["d"])) / (2 * h)
+            assert abs(fd - grad[idx]) <= 1e-6 * max(1.0, abs(fd)), (which, idx, fd, grad[idx])
+
+
+def test_invalid_arguments_rejected(restatement):
+    a, b, c, d = make_system([4, 4], 0)
+    with pytest.raises(ValueError):
+        restatement.strided_batch(a, b, c, d, [4, 4], 2)

@@ -1,0 +1,13 @@
+"""tridsolver_b200 — B200-native batched scalar tridiagonal solver.
+
+The product is the C-ABI library lib/libtridsolver_b200.so (sm_100a kernels
+behind the reference's tridDmtsvStridedBatch / tridSmtsvStridedBatch (+Inc)
+entry points, include/tridsolver.h). This package binds it for Python.
+"""
+
+from .api import (  # noqa: F401
+    FAMILY_AUTO, FAMILY_HYBRID, FAMILY_LONG, FAMILY_PCR, TridError, TridParams, TridStatus,
+    describe_plan, force_plan, get_blocking, launch_count, on_stream, pivot_status,
+    set_blocking, set_stream, solve, strided_batch, tridDmtsvStridedBatch,
+    tridDmtsvStridedBatchInc, tridSmtsvStridedBatch, tridSmtsvStridedBatchInc)
+from ._lib import LIB_PATH, load as load_library  # noqa: F401

@@ -1,0 +1,205 @@
+"""Python mirror of the reference's C API, over the in-tree C-ABI library.
+
+Two levels:
+
+* The reference's four entry points under their own names
+  (tridDmtsvStridedBatch, tridSmtsvStridedBatch, ...Inc), taking device
+  pointers (ints) or CUDA tensors, returning the tridStatus_t code exactly as
+  the C functions do (scalar/include/tridsolver.h:39-69). These are blocking
+  by default, like the reference.
+* ``strided_batch`` / ``solve``: the same solve on torch CUDA tensors,
+  enqueued on torch's current stream without blocking, raising TridError on
+  a non-success status.
+
+Layout is the reference's: element (i0, i1, i2) at i0 + i1*pads[0] +
+i2*pads[0]*pads[1]. A C-contiguous torch tensor of shape (n2, n1, n0) has
+exactly that layout with dims = [n0, n1, n2], so torch dimension k is the
+reference's solvedim = ndim - 1 - k.
+"""
+
+import ctypes
+import enum
+
+from . import _lib
+
+
+class TridStatus(enum.IntEnum):
+    """tridStatus_t (scalar/include/trid_common.h:64-75)."""
+    SUCCESS = 0
+    NOT_INITIALIZED = 1
+    ALLOC_FAILED = 2
+    INVALID_VALUE = 3
+    ARCH_MISMATCH = 4
+    MAPPING_ERROR = 5
+    EXECUTION_FAILED = 6
+    INTERNAL_ERROR = 7
+    MATRIX_TYPE_NOT_SUPPORTED = 8
+    ZERO_PIVOT = 9
+
+
+class TridError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = TridStatus(status)
+        super().__init__(f"{what}: {self.status.name}" if what else self.status.name)
+
+
+MAXDIM = 3
+
+
+class TridParams(ctypes.Structure):
+    """struct TridParams (scalar/include/trid_params.h:31-35)."""
+    _fields_ = [("mpi_params", ctypes.c_void_p),
+                ("opts", ctypes.c_int * MAXDIM),
+                ("sync", ctypes.c_int)]
+
+
+FAMILY_AUTO, FAMILY_HYBRID, FAMILY_PCR, FAMILY_LONG = -1, 0, 1, 2
+
+
+def _addr(x):
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return int(x)
+
+
+def _ctx(ctx):
+    if ctx is None:
+        return None
+    if isinstance(ctx, TridParams):
+        return ctypes.addressof(ctx)
+    return int(ctx)
+
+
+def _ints(vals):
+    vals = list(vals)
+    return (ctypes.c_int * max(1, len(vals)))(*[int(v) for v in vals])
+
+
+# ---- the reference's entry points ------------------------------------------
+
+def tridDmtsvStridedBatch(ctx, a, b, c, d, ndim, solvedim, dims, pads):
+    return _lib.load().tridDmtsvStridedBatch(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                             int(ndim), int(solvedim), _ints(dims), _ints(pads))
+
+
+def tridSmtsvStridedBatch(ctx, a, b, c, d, ndim, solvedim, dims, pads):
+    return _lib.load().tridSmtsvStridedBatch(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                             int(ndim), int(solvedim), _ints(dims), _ints(pads))
+
+
+def tridDmtsvStridedBatchInc(ctx, a, b, c, d, u, ndim, solvedim, dims, pads):
+    return _lib.load().tridDmtsvStridedBatchInc(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                                _addr(u), int(ndim), int(solvedim), _ints(dims),
+                                                _ints(pads))
+
+
+def tridSmtsvStridedBatchInc(ctx, a, b, c, d, u, ndim, solvedim, dims, pads):
+    return _lib.load().tridSmtsvStridedBatchInc(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                                _addr(u), int(ndim), int(solvedim), _ints(dims),
+                                                _ints(pads))
+
+
+# ---- execution control -------------------------------------------------------
+
+def set_stream(stream):
+    """stream: a torch.cuda.Stream, a raw cudaStream_t (int) or None."""
+    raw = getattr(stream, "cuda_stream", stream)
+    _lib.load().tridSetStream(None if raw in (None, 0) else int(raw))
+
+
+def set_blocking(blocking):
+    _lib.load().tridSetBlocking(1 if blocking else 0)
+
+
+def get_blocking():
+    return bool(_lib.load().tridGetBlocking())
+
+
+def pivot_status():
+    return TridStatus(_lib.load().tridGetPivotStatus())
+
+
+def launch_count():
+    return int(_lib.load().tridGetLaunchCount())
+
+
+def force_plan(family=FAMILY_AUTO, rows_per_thread=0):
+    st = _lib.load().tridForcePlan(int(family), int(rows_per_thread))
+    if st != 0:
+        raise TridError(st, "tridForcePlan")
+
+
+def describe_plan(dtype_bytes, dims, solvedim, pads=None):
+    pads = dims if pads is None else pads
+    buf = ctypes.create_string_buffer(128)
+    n = _lib.load().tridDescribePlan(int(dtype_bytes), len(dims), int(solvedim), _ints(dims),
+                                     _ints(pads), buf, 128)
+    if n < 0:
+        raise TridError(TridStatus.INVALID_VALUE, "tridDescribePlan")
+    return buf.value.decode()
+
+
+class on_stream:
+    """Context manager: run library calls on `stream` (default: torch's current
+    stream) with the given blocking mode, restoring the previous settings."""
+
+    def __init__(self, stream=None, blocking=False):
+        self.stream = stream
+        self.blocking = blocking
+
+    def __enter__(self):
+        import torch
+        lib = _lib.load()
+        self._prev = (lib.tridGetStream(), lib.tridGetBlocking())
+        s = self.stream if self.stream is not None else torch.cuda.current_stream()
+        set_stream(s)
+        set_blocking(self.blocking)
+        return self
+
+    def __exit__(self, *exc):
+        lib = _lib.load()
+        lib.tridSetStream(self._prev[0])
+        lib.tridSetBlocking(self._prev[1])
+        return False
+
+
+# ---- torch-tensor interface ------------------------------------------------------
+
+def strided_batch(a, b, c, d, solvedim, dims, pads=None, u=None, ctx=None):
+    """Solve along `solvedim` of the reference layout on CUDA tensors (any shape,
+    addressed through dims/pads from their first element). d <- x, or u += x
+    when u is given. Enqueued on torch's current stream; raises TridError."""
+    import torch
+    pads = list(dims) if pads is None else list(pads)
+    dt = d.dtype
+    if dt not in (torch.float64, torch.float32):
+        raise TypeError("float32 or float64 tensors only")
+    for t in (a, b, c, d) + ((u,) if u is not None else ()):
+        if t.dtype != dt or not t.is_cuda:
+            raise TypeError("all arrays must be CUDA tensors of one dtype")
+    with torch.cuda.device(d.device), on_stream(blocking=False):
+        if dt == torch.float64:
+            st = (tridDmtsvStridedBatch(ctx, a, b, c, d, len(dims), solvedim, dims, pads) if u is None
+                  else tridDmtsvStridedBatchInc(ctx, a, b, c, d, u, len(dims), solvedim, dims, pads))
+        else:
+            st = (tridSmtsvStridedBatch(ctx, a, b, c, d, len(dims), solvedim, dims, pads) if u is None
+                  else tridSmtsvStridedBatchInc(ctx, a, b, c, d, u, len(dims), solvedim, dims, pads))
+    if st != 0:
+        raise TridError(st, "strided batch solve")
+
+
+def solve(a, b, c, d, dim=-1, u=None):
+    """Solve along torch dimension `dim` of C-contiguous tensors of one shape
+    (ndim <= 3). d <- x in place, or u += x when u is given."""
+    shape = tuple(d.shape)
+    nd = len(shape)
+    if not 1 <= nd <= MAXDIM:
+        raise ValueError("1 to 3 dimensions")
+    for t in (a, b, c, d) + ((u,) if u is not None else ()):
+        if tuple(t.shape) != shape or not t.is_contiguous():
+            raise ValueError("contiguous tensors of one shape")
+    dims = list(reversed(shape))
+    solvedim = nd - 1 - (dim % nd)
+    strided_batch(a, b, c, d, solvedim, dims, dims, u=u)

@@ -1,0 +1,266 @@
+// The C ABI of libtridsolver_b200: the reference's four strided-batch entry
+// points (scalar/include/tridsolver.h:39-69) and the extensions declared in
+// include/tridsolver_b200.h.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "trid_internal.h"
+#include "tridsolver.h"
+
+namespace trid {
+
+Settings &settings() {
+  static thread_local Settings s;
+  return s;
+}
+
+// ---- zero-pivot record: one host-mapped word per device -------------------
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_flag_mu;
+unsigned *g_flag_host = nullptr;     // kMaxDevices words, mapped
+unsigned *g_flag_dev[kMaxDevices] = {};
+bool g_flag_tried = false;
+}  // namespace
+
+unsigned *pivot_flag_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lk(g_flag_mu);
+  if (!g_flag_tried) {
+    g_flag_tried = true;
+    void *h = nullptr;
+    if (cudaHostAlloc(&h, kMaxDevices * sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable) ==
+        cudaSuccess) {
+      memset(h, 0, kMaxDevices * sizeof(unsigned));
+      g_flag_host = static_cast<unsigned *>(h);
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (!g_flag_host) return nullptr;
+  if (!g_flag_dev[dev]) {
+    void *dp = nullptr;
+    if (cudaHostGetDevicePointer(&dp, g_flag_host + dev, 0) == cudaSuccess)
+      g_flag_dev[dev] = static_cast<unsigned *>(dp);
+    else
+      cudaGetLastError();
+  }
+  return g_flag_dev[dev];
+}
+
+bool pivot_flag_take() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || !g_flag_host) return false;
+  volatile unsigned *w = g_flag_host + dev;
+  unsigned v = *w;
+  if (v) *w = 0u;
+  return v != 0;
+}
+
+// ---- device check ----------------------------------------------------------
+static tridStatus_t check_device() {
+  static thread_local int checked_dev = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return TRID_STATUS_NOT_INITIALIZED;
+  }
+  if (dev == checked_dev) return TRID_STATUS_SUCCESS;
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return TRID_STATUS_NOT_INITIALIZED;
+  }
+  if (major != 10) return TRID_STATUS_ARCH_MISMATCH;  // built for sm_100a only
+  checked_dev = dev;
+  return TRID_STATUS_SUCCESS;
+}
+
+tridStatus_t status_of(cudaError_t e) {
+  switch (e) {
+    case cudaSuccess: return TRID_STATUS_SUCCESS;
+    case cudaErrorMemoryAllocation: return TRID_STATUS_ALLOC_FAILED;
+    case cudaErrorNoKernelImageForDevice:
+    case cudaErrorInvalidDeviceFunction: return TRID_STATUS_ARCH_MISMATCH;
+    default: return TRID_STATUS_EXECUTION_FAILED;
+  }
+}
+
+// Validates the strided-batch arguments and fills a BatchArgs. Returns
+// SUCCESS with *empty = true when there is nothing to solve.
+template <typename R>
+static tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, bool inc, int ndim,
+                               int solvedim, const int *dims_p, const int *pads_p,
+                               BatchArgs<R> *out, bool *empty) {
+  if (ndim < 1 || ndim > MAXDIM || solvedim < 0 || solvedim >= ndim || !dims_p || !pads_p)
+    return TRID_STATUS_INVALID_VALUE;
+  long long dims[3] = {1, 1, 1}, pads[3] = {1, 1, 1};
+  for (int i = 0; i < ndim; ++i) {
+    if (dims_p[i] < 0) return TRID_STATUS_INVALID_VALUE;
+    dims[i] = dims_p[i];
+    pads[i] = pads_p[i];
+    // the padded extent of every dimension that enters the index arithmetic
+    // must cover its size
+    if (i < ndim - 1 && pads[i] < dims[i]) return TRID_STATUS_INVALID_VALUE;
+  }
+  *empty = dims[0] * dims[1] * dims[2] == 0;
+  if (*empty) return TRID_STATUS_SUCCESS;
+  if (!a || !b || !c || !d || (inc && !u)) return TRID_STATUS_INVALID_VALUE;
+  if (dims[solvedim] > 0x7fffffffLL) return TRID_STATUS_INVALID_VALUE;
+  BatchArgs<R> p{};
+  p.a = a;
+  p.b = b;
+  p.c = c;
+  p.d_in = d;
+  p.d_out = d;
+  p.u = inc ? u : nullptr;
+  p.N = (int)dims[solvedim];
+  const long long s01 = pads[0] * pads[1];
+  if (solvedim == 0) {
+    p.n0 = dims[1];
+    p.nsys = dims[1] * dims[2];
+    p.st0 = pads[0];
+    p.st1 = s01;
+    p.stride = 1;
+  } else if (solvedim == 1) {
+    p.n0 = dims[0];
+    p.nsys = dims[0] * dims[2];
+    p.st0 = 1;
+    p.st1 = s01;
+    p.stride = pads[0];
+  } else {
+    p.n0 = dims[0];
+    p.nsys = dims[0] * dims[1];
+    p.st0 = 1;
+    p.st1 = pads[0];
+    p.stride = s01;
+  }
+  *out = p;
+  return TRID_STATUS_SUCCESS;
+}
+
+template <typename R, bool INC>
+static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b, const R *c, R *d,
+                                  R *u, int ndim, int solvedim, const int *dims, const int *pads) {
+  (void)ctx;  // opts are hints; the autotuned plan is used for every value
+  BatchArgs<R> p;
+  bool empty = false;
+  tridStatus_t st = make_batch<R>(a, b, c, d, u, INC, ndim, solvedim, dims, pads, &p, &empty);
+  if (st != TRID_STATUS_SUCCESS || empty) return st;
+  st = check_device();
+  if (st != TRID_STATUS_SUCCESS) return st;
+  const Settings &cfg = settings();
+  p.flag = pivot_flag_device();
+  if (cfg.blocking) pivot_flag_take();  // report only this call's pivots
+  const Plan plan = choose_plan<R>(p, vec_aligned<R>(p));
+  cudaError_t e = launch_batch<R, INC>(p, plan, cfg.stream);
+  if (e != cudaSuccess) return status_of(e);
+  if (cfg.blocking) {
+    e = cudaStreamSynchronize(cfg.stream);
+    if (e != cudaSuccess) return status_of(e);
+    if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
+}  // namespace trid
+
+using namespace trid;
+
+EXTERN_C tridStatus_t tridDmtsvStridedBatch(const TridParams *ctx, const double *a, const double *b,
+                                            const double *c, double *d, int ndim, int solvedim,
+                                            const int *dims, const int *pads) {
+  return solve_strided<double, false>(ctx, a, b, c, d, nullptr, ndim, solvedim, dims, pads);
+}
+
+EXTERN_C tridStatus_t tridSmtsvStridedBatch(const TridParams *ctx, const float *a, const float *b,
+                                            const float *c, float *d, int ndim, int solvedim,
+                                            const int *dims, const int *pads) {
+  return solve_strided<float, false>(ctx, a, b, c, d, nullptr, ndim, solvedim, dims, pads);
+}
+
+EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const TridParams *ctx, const double *a,
+                                               const double *b, const double *c, double *d,
+                                               double *u, int ndim, int solvedim, const int *dims,
+                                               const int *pads) {
+  return solve_strided<double, true>(ctx, a, b, c, d, u, ndim, solvedim, dims, pads);
+}
+
+EXTERN_C tridStatus_t tridSmtsvStridedBatchInc(const TridParams *ctx, const float *a,
+                                               const float *b, const float *c, float *d, float *u,
+                                               int ndim, int solvedim, const int *dims,
+                                               const int *pads) {
+  return solve_strided<float, true>(ctx, a, b, c, d, u, ndim, solvedim, dims, pads);
+}
+
+// ---- extensions -------------------------------------------------------------
+
+EXTERN_C tridStatus_t tridSetStream(void *cuda_stream) {
+  settings().stream = static_cast<cudaStream_t>(cuda_stream);
+  return TRID_STATUS_SUCCESS;
+}
+
+EXTERN_C void *tridGetStream(void) { return settings().stream; }
+
+EXTERN_C tridStatus_t tridSetBlocking(int blocking) {
+  settings().blocking = blocking != 0;
+  return TRID_STATUS_SUCCESS;
+}
+
+EXTERN_C int tridGetBlocking(void) { return settings().blocking ? 1 : 0; }
+
+EXTERN_C tridStatus_t tridGetPivotStatus(void) {
+  return pivot_flag_take() ? TRID_STATUS_ZERO_PIVOT : TRID_STATUS_SUCCESS;
+}
+
+EXTERN_C unsigned long long tridGetLaunchCount(void) { return g_launches.load(); }
+
+EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread) {
+  Settings &s = settings();
+  if (family < 0) {
+    s.force_family = TRID_FAMILY_AUTO;
+    s.force_m = 0;
+    return TRID_STATUS_SUCCESS;
+  }
+  if (family > TRID_FAMILY_LONG) return TRID_STATUS_INVALID_VALUE;
+  const int m = rows_per_thread;
+  if (family == TRID_FAMILY_HYBRID && !(m == 0 || m == 2 || m == 4 || m == 8 || m == 16 || m == 32))
+    return TRID_STATUS_INVALID_VALUE;
+  if (family == TRID_FAMILY_LONG && !(m == 0 || m == 8 || m == 16)) return TRID_STATUS_INVALID_VALUE;
+  s.force_family = family;
+  s.force_m = m;
+  return TRID_STATUS_SUCCESS;
+}
+
+EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                              const int *pads, char *buf, int buflen) {
+  std::string desc;
+  bool empty = false;
+  // alignment is taken as satisfied: the description is of the shape only
+  if (dtype_bytes == 8) {
+    BatchArgs<double> p;
+    double *dummy = reinterpret_cast<double *>(256);
+    if (make_batch<double>(dummy, dummy, dummy, dummy, nullptr, false, ndim, solvedim, dims, pads,
+                           &p, &empty) != TRID_STATUS_SUCCESS)
+      return -1;
+    desc = empty ? "empty" : choose_plan<double>(p, vec_aligned<double>(p)).describe();
+  } else if (dtype_bytes == 4) {
+    BatchArgs<float> p;
+    float *dummy = reinterpret_cast<float *>(256);
+    if (make_batch<float>(dummy, dummy, dummy, dummy, nullptr, false, ndim, solvedim, dims, pads, &p,
+                          &empty) != TRID_STATUS_SUCCESS)
+      return -1;
+    desc = empty ? "empty" : choose_plan<float>(p, vec_aligned<float>(p)).describe();
+  } else {
+    return -1;
+  }
+  if (buf && buflen > 0) {
+    strncpy(buf, desc.c_str(), (size_t)buflen - 1);
+    buf[buflen - 1] = '\0';
+  }
+  return (int)desc.size();
+}

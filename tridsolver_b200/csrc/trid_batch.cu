@@ -1,0 +1,197 @@
+// Plan selection and launchers of the batched solve kernels.
+#include <cstdio>
+#include <string>
+
+#include "trid_internal.h"
+
+namespace trid {
+
+std::atomic<unsigned long long> g_launches{0};
+
+std::string Plan::describe() const {
+  char buf[96];
+  const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
+  snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W, vec ? " vec" : "");
+  return buf;
+}
+
+static int pow2_ceil(long long v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+template <typename R>
+bool vec_aligned(const BatchArgs<R> &p) {
+  if (p.stride != 1) return false;
+  auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+  if (!al(p.a) || !al(p.b) || !al(p.c) || !al(p.d_in) || !al(p.d_out)) return false;
+  if (p.u && !al(p.u)) return false;
+  if ((p.st0 * (long long)sizeof(R)) % 16 || (p.st1 * (long long)sizeof(R)) % 16) return false;
+  return true;
+}
+
+// Largest system the single-warp hybrid holds: 32 lanes x M_max rows, with
+// M_max = 16 (double) or 32 (float) so a lane's chunk state stays in
+// registers without spilling.
+template <typename R> constexpr int warp_max_rows() { return sizeof(R) == 8 ? 512 : 1024; }
+
+// Built-in table: rows per thread by system length (see DESIGN.md for the
+// measurements behind it).
+template <typename R>
+static int default_m(int N) {
+  if (N <= 256) return 8;
+  if (N <= 512) return 16;
+  return 32;
+}
+
+template <typename R>
+Plan choose_plan(const BatchArgs<R> &p, bool aligned16) {
+  const Settings &st = settings();
+  Plan plan;
+  const int N = p.N;
+  int fam = st.force_family;
+  int M = st.force_m;
+  if (fam == TRID_FAMILY_AUTO) fam = N > warp_max_rows<R>() ? TRID_FAMILY_LONG : TRID_FAMILY_HYBRID;
+  if (fam == TRID_FAMILY_PCR && N > 32) fam = TRID_FAMILY_HYBRID;
+  if (fam == TRID_FAMILY_HYBRID && M == 0) M = default_m<R>(N);
+  if (fam == TRID_FAMILY_HYBRID && (long long)M * 32 < N) fam = TRID_FAMILY_LONG, M = 0;
+  plan.family = fam;
+  if (fam == TRID_FAMILY_PCR) {
+    plan.M = 1;
+    plan.T = pow2_ceil(N < 1 ? 1 : N);
+    return plan;
+  }
+  if (fam == TRID_FAMILY_LONG) {
+    plan.M = (M == 8 || M == 16) ? M : 16;
+    return plan;
+  }
+  plan.M = M;
+  plan.T = pow2_ceil((N + M - 1) / M);
+  if (p.stride == 1) {
+    plan.vec = aligned16 && ((M * (int)sizeof(R)) % 16 == 0);
+  } else {
+    int W = 256 / plan.T;
+    const int wmin = 32 / plan.T > 1 ? 32 / plan.T : 1;
+    const int n0p = pow2_ceil(p.n0);
+    if (W > n0p) W = n0p;
+    if (W < wmin) W = wmin;
+    plan.W = W;
+  }
+  return plan;
+}
+
+// ---------------------------------------------------------------------------
+
+template <typename R, int M, bool INC>
+static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  if (p.stride == 1) {
+    const int threads = 128;
+    const long long total = p.nsys * plan.T;
+    const long long blocks = (total + threads - 1) / threads;
+    if (plan.vec) {
+      if constexpr ((M * sizeof(R)) % 16 == 0) {
+        contig_kernel<R, M, INC, true><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
+      } else {
+        return cudaErrorInvalidValue;
+      }
+    } else {
+      contig_kernel<R, M, INC, false><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
+    }
+  } else {
+    const int threads = plan.W * plan.T;
+    const long long ngx = (p.n0 + plan.W - 1) / plan.W;
+    const long long n1 = p.nsys / p.n0;
+    const long long blocks = ngx * n1;
+    const size_t smem = (size_t)6 * plan.T * (plan.W + 1) * sizeof(R);
+    strided_kernel<R, M, INC><<<(unsigned)blocks, threads, smem, st>>>(p, plan.T, plan.W, ngx);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+template <typename R, bool INC>
+static cudaError_t launch_hybrid(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  switch (plan.M) {
+    case 2: return launch_hybrid_m<R, 2, INC>(p, plan, st);
+    case 4: return launch_hybrid_m<R, 4, INC>(p, plan, st);
+    case 8: return launch_hybrid_m<R, 8, INC>(p, plan, st);
+    case 16: return launch_hybrid_m<R, 16, INC>(p, plan, st);
+    case 32: return launch_hybrid_m<R, 32, INC>(p, plan, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename R, bool INC>
+static cudaError_t launch_pcr(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  const int threads = 128;
+  const long long total = p.nsys * plan.T;
+  const long long blocks = (total + threads - 1) / threads;
+  pcr_kernel<R, INC><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+template <typename R, int M, bool INC>
+static cudaError_t launch_long_m(const BatchArgs<R> &p, cudaStream_t st) {
+  const long long nc = ((long long)p.N + M - 1) / M;
+  const long long nred = p.nsys * 2 * nc;
+  R *scratch = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&scratch, (size_t)nred * 4 * sizeof(R), st);
+  if (e != cudaSuccess) return e;
+  R *ra = scratch, *rb = ra + nred, *rc = rb + nred, *rd = rc + nred;
+  const int threads = 128;
+  const long long items = p.nsys * nc;
+  const long long blocks = (items + threads - 1) / threads;
+  long_reduce_kernel<R, M><<<(unsigned)blocks, threads, 0, st>>>(p, nc, ra, rb, rc, rd);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    BatchArgs<R> q{};
+    q.a = ra;
+    q.b = rb;
+    q.c = rc;
+    q.d_in = rd;
+    q.d_out = rd;
+    q.u = nullptr;
+    q.N = (int)(2 * nc);
+    q.nsys = p.nsys;
+    q.n0 = p.nsys;
+    q.st0 = 2 * nc;
+    q.st1 = 0;
+    q.stride = 1;
+    q.flag = p.flag;
+    Plan qp = choose_plan<R>(q, vec_aligned<R>(q));
+    e = launch_batch<R, false>(q, qp, st);
+  }
+  if (e == cudaSuccess) {
+    long_substitute_kernel<R, M, INC><<<(unsigned)blocks, threads, 0, st>>>(p, nc, rd);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    e = cudaGetLastError();
+  }
+  cudaError_t ef = cudaFreeAsync(scratch, st);
+  return e != cudaSuccess ? e : ef;
+}
+
+template <typename R, bool INC>
+cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  if (p.nsys <= 0 || p.N <= 0) return cudaSuccess;
+  switch (plan.family) {
+    case TRID_FAMILY_PCR: return launch_pcr<R, INC>(p, plan, st);
+    case TRID_FAMILY_LONG:
+      return plan.M == 8 ? launch_long_m<R, 8, INC>(p, st) : launch_long_m<R, 16, INC>(p, st);
+    default: return launch_hybrid<R, INC>(p, plan, st);
+  }
+}
+
+#define INSTANTIATE(R)                                                                  \
+  template Plan choose_plan<R>(const BatchArgs<R> &, bool);                           \
+  template bool vec_aligned<R>(const BatchArgs<R> &);                                 \
+  template cudaError_t launch_batch<R, false>(const BatchArgs<R> &, const Plan &,     \
+                                              cudaStream_t);                          \
+  template cudaError_t launch_batch<R, true>(const BatchArgs<R> &, const Plan &, cudaStream_t);
+
+INSTANTIATE(float)
+INSTANTIATE(double)
+
+}  // namespace trid

@@ -1,0 +1,51 @@
+// Host-side internals shared by the translation units of libtridsolver_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <string>
+
+#include "trid_kernels.cuh"
+#include "tridsolver_b200.h"
+
+namespace trid {
+
+struct Plan {
+  int family = TRID_FAMILY_HYBRID;  // TRID_FAMILY_*
+  int M = 8;                        // rows per thread (hybrid, long)
+  int T = 1;                        // threads per system (hybrid, pcr)
+  int W = 1;                        // systems per block (strided hybrid)
+  bool vec = false;                 // 16-byte vector loads (contiguous hybrid)
+  std::string describe() const;
+};
+
+// Per-thread execution settings (see tridsolver_b200.h).
+struct Settings {
+  cudaStream_t stream = nullptr;
+  bool blocking = true;
+  int force_family = TRID_FAMILY_AUTO;
+  int force_m = 0;
+};
+Settings &settings();
+
+extern std::atomic<unsigned long long> g_launches;
+
+// Host-mapped zero-pivot word of the current device (device pointer), or
+// nullptr if it could not be set up.
+unsigned *pivot_flag_device();
+bool pivot_flag_take();  // reads and clears the word of the current device
+
+template <typename R>
+Plan choose_plan(const BatchArgs<R> &p, bool aligned16);
+
+// Enqueues the solve of batch p on `st` (no synchronisation).
+template <typename R, bool INC>
+cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
+
+// Whether every pointer and every system start allows 16-byte vector access
+// (contiguous systems only).
+template <typename R>
+bool vec_aligned(const BatchArgs<R> &p);
+
+}  // namespace trid

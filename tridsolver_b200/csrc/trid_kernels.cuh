@@ -1,0 +1,300 @@
+// Kernel templates of the batched tridiagonal solve.
+//
+// A batch is described by BatchArgs: system s = i0 + n0*i1 starts at element
+// i0*st0 + i1*st1 and its rows are `stride` elements apart. The strided-batch
+// API maps onto it as (p = pads):
+//   solvedim 0:  i0 = y, i1 = z,  st0 = p0, st1 = p0*p1, stride = 1
+//   solvedim 1:  i0 = x, i1 = z,  st0 = 1,  st1 = p0*p1, stride = p0
+//   solvedim 2:  i0 = x, i1 = y,  st0 = 1,  st1 = p0,    stride = p0*p1
+// (the reference's index arithmetic, scalar/src/cpu/trid_cpu.cpp:369-454).
+//
+// Families (all keep each element in registers between one read and one
+// write of HBM; see trid_device.cuh for the algorithm):
+//   contig_kernel   stride == 1: T consecutive lanes own the T chunks of one
+//                   system, so the reduced solve is all warp shuffles and the
+//                   M rows of a lane are contiguous (16-byte vector loads when
+//                   aligned).
+//   strided_kernel  stride > 1: a block is W neighbouring systems x T chunks
+//                   with the system index fastest, so every warp load reads
+//                   W contiguous elements of one row; the reduced rows are
+//                   re-dealt through shared memory so each system's T chunks
+//                   land in one warp segment for the shuffle solve.
+//   pcr_kernel      M = 1: one row per lane, pure PCR (systems <= 32 rows).
+//   long_*_kernel   systems longer than one warp can hold: chunk
+//                   elimination writes two reduced rows per chunk to scratch,
+//                   the reduced batch is solved recursively as a contiguous
+//                   batch, then every chunk is eliminated again from its inputs
+//                   and substituted.
+#pragma once
+
+#include "trid_device.cuh"
+
+namespace trid {
+
+template <typename R> struct BatchArgs {
+  const R *a, *b, *c;
+  const R *d_in;  // right-hand side (== d_out unless INC)
+  R *d_out;       // x is written here when !INC
+  R *u;           // u += x when INC
+  int N;          // rows per system
+  long long nsys;
+  long long n0;   // systems along the fastest enumerating dimension
+  long long st0, st1, stride;
+  unsigned *flag;  // host-mapped zero-pivot word (may be null)
+};
+
+template <typename R>
+__device__ __forceinline__ long long sys_base(const BatchArgs<R> &p, long long s) {
+  long long i1 = s / p.n0;
+  long long i0 = s - i1 * p.n0;
+  return i0 * p.st0 + i1 * p.st1;
+}
+
+// Loads chunk rows [row0, row0+M) of a system starting at `base` into
+// registers, identity rows past N, a[0] and c[N-1] forced to zero.
+template <typename R, int M, bool VEC>
+__device__ __forceinline__ void load_chunk(const BatchArgs<R> &p, long long base, int row0,
+                                           bool active, R (&ra)[M], R (&rb)[M], R (&rc)[M],
+                                           R (&rd)[M]) {
+  const int N = p.N;
+  if (VEC && active && row0 + M <= N) {
+    const long long o = base + row0;  // stride == 1 for VEC
+    load_vec<R, M>(p.a + o, ra);
+    load_vec<R, M>(p.b + o, rb);
+    load_vec<R, M>(p.c + o, rc);
+    load_vec<R, M>(p.d_in + o, rd);
+  } else {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int row = row0 + i;
+      if (active && row < N) {
+        const long long o = base + (long long)row * p.stride;
+        ra[i] = __ldg(p.a + o);
+        rb[i] = __ldg(p.b + o);
+        rc[i] = __ldg(p.c + o);
+        rd[i] = __ldg(p.d_in + o);
+      } else {
+        ra[i] = R(0);
+        rb[i] = R(1);
+        rc[i] = R(0);
+        rd[i] = R(0);
+      }
+    }
+  }
+  if (row0 == 0) ra[0] = R(0);
+#pragma unroll
+  for (int i = 0; i < M; ++i)
+    if (row0 + i == N - 1) rc[i] = R(0);
+}
+
+// Writes x (in rd) for rows [row0, row0+M) that lie inside the system.
+template <typename R, int M, bool INC, bool VEC>
+__device__ __forceinline__ void store_chunk(const BatchArgs<R> &p, long long base, int row0,
+                                            bool active, const R (&x)[M]) {
+  if (!active) return;
+  const int N = p.N;
+  if (VEC && row0 + M <= N) {
+    const long long o = base + row0;
+    if (INC) {
+      R uu[M];
+      load_vec<R, M>(p.u + o, uu);
+#pragma unroll
+      for (int i = 0; i < M; ++i) uu[i] += x[i];
+      store_vec<R, M>(p.u + o, uu);
+    } else {
+      store_vec<R, M>(p.d_out + o, x);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int row = row0 + i;
+      if (row < N) {
+        const long long o = base + (long long)row * p.stride;
+        if (INC)
+          p.u[o] += x[i];
+        else
+          p.d_out[o] = x[i];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// contig_kernel: stride == 1, T lanes per system (T | 32), 32/T systems per
+// warp. Block size is a multiple of 32.
+template <typename R, int M, bool INC, bool VEC>
+__global__ void __launch_bounds__(128) contig_kernel(const BatchArgs<R> p, int T) {
+  const int t = threadIdx.x & (T - 1);
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long s = gtid / T;
+  const bool active = s < p.nsys;
+  const long long base = active ? sys_base(p, s) : 0;
+  const int row0 = t * M;
+  R ra[M], rb[M], rc[M], rd[M];
+  load_chunk<R, M, VEC>(p, base, row0, active, ra, rb, rc, rd);
+  bool bad = false;
+  chunk_forward<R, M>(ra, rb, rc, rd, bad);
+  chunk_backward<R, M>(ra, rc, rd, bad);
+  Row<R> top{ra[0], rc[0], rd[0]};
+  Row<R> bot{ra[M - 1], rc[M - 1], rd[M - 1]};
+  R y, z;
+  reduced_solve<R>(top, bot, t, T, y, z, bad);
+  chunk_substitute<R, M>(ra, rc, rd, y, z);
+  store_chunk<R, M, INC, VEC>(p, base, row0, active, rd);
+  report_bad_pivot(bad && active, p.flag);
+}
+
+// ---------------------------------------------------------------------------
+// strided_kernel: block = W systems (neighbouring i0) x T chunks, thread
+// (s, t) = (tid % W, tid / W). W*T is a multiple of 32.
+template <typename R, int M, bool INC>
+__global__ void __launch_bounds__(256) strided_kernel(const BatchArgs<R> p, int T, int W,
+                                                      long long ngx) {
+  extern __shared__ unsigned char smem_raw[];
+  R *sm = reinterpret_cast<R *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int s = tid % W;
+  const int t = tid / W;
+  const long long gx = blockIdx.x % ngx;
+  const long long i1 = blockIdx.x / ngx;
+  const long long i0 = gx * W + s;
+  const bool active = i0 < p.n0;
+  const long long base = i0 * p.st0 + i1 * p.st1;
+  const int row0 = t * M;
+  R ra[M], rb[M], rc[M], rd[M];
+  load_chunk<R, M, false>(p, base, row0, active, ra, rb, rc, rd);
+  bool bad = false;
+  chunk_forward<R, M>(ra, rb, rc, rd, bad);
+  chunk_backward<R, M>(ra, rc, rd, bad);
+
+  // re-deal the reduced rows: slot (t, s) at t*(W+1)+s, six values each
+  const int ld = W + 1;
+  const int nslot = T * ld;
+  {
+    const int k = t * ld + s;
+    sm[0 * nslot + k] = ra[0];
+    sm[1 * nslot + k] = rc[0];
+    sm[2 * nslot + k] = rd[0];
+    sm[3 * nslot + k] = ra[M - 1];
+    sm[4 * nslot + k] = rc[M - 1];
+    sm[5 * nslot + k] = rd[M - 1];
+  }
+  __syncthreads();
+  {
+    const int s2 = tid / T;
+    const int t2 = tid & (T - 1);
+    const int k = t2 * ld + s2;
+    Row<R> top{sm[0 * nslot + k], sm[1 * nslot + k], sm[2 * nslot + k]};
+    Row<R> bot{sm[3 * nslot + k], sm[4 * nslot + k], sm[5 * nslot + k]};
+    R y, z;
+    reduced_solve<R>(top, bot, t2, T, y, z, bad);
+    // slot k is read and rewritten by this thread only
+    sm[0 * nslot + k] = y;
+    sm[1 * nslot + k] = z;
+  }
+  __syncthreads();
+  const int k = t * ld + s;
+  const R y = sm[0 * nslot + k];
+  const R z = sm[1 * nslot + k];
+  chunk_substitute<R, M>(ra, rc, rd, y, z);
+  store_chunk<R, M, INC, false>(p, base, row0, active, rd);
+  report_bad_pivot(bad && active, p.flag);
+}
+
+// ---------------------------------------------------------------------------
+// pcr_kernel: one row per lane, T lanes per system (N <= T <= 32). For
+// stride == 1 the lanes of a system read consecutive elements; for strided
+// batches the lane order is still row-major inside the system, which is the
+// right trade only for short systems.
+template <typename R, bool INC>
+__global__ void __launch_bounds__(128) pcr_kernel(const BatchArgs<R> p, int T) {
+  const int t = threadIdx.x & (T - 1);
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long s = gtid / T;
+  const bool active = s < p.nsys && t < p.N;
+  const long long o = (s < p.nsys ? sys_base(p, s) : 0) + (long long)t * p.stride;
+  R a = R(0), b = R(1), c = R(0), d = R(0);
+  if (active) {
+    a = t == 0 ? R(0) : __ldg(p.a + o);
+    b = __ldg(p.b + o);
+    c = t == p.N - 1 ? R(0) : __ldg(p.c + o);
+    d = __ldg(p.d_in + o);
+  }
+  bool bad = false;
+  R x = pcr_solve<R>(a, b, c, d, t, T, bad);
+  if (active) {
+    if (INC)
+      p.u[o] += x;
+    else
+      p.d_out[o] = x;
+  }
+  report_bad_pivot(bad && active, p.flag);
+}
+
+// ---------------------------------------------------------------------------
+// Long systems. Work item = (system, chunk); for stride == 1 the chunk index
+// is fastest (neighbouring lanes read neighbouring chunks), otherwise i0 is
+// fastest (neighbouring lanes read neighbouring systems, coalesced).
+// Reduced system of system s: rows [s*2nc, s*2nc + 2nc) of ra/rb/rc/rd.
+template <typename R>
+__device__ __forceinline__ void long_item(const BatchArgs<R> &p, long long item, long long nc,
+                                          long long &s, long long &chunk) {
+  if (p.stride == 1) {
+    s = item / nc;
+    chunk = item - s * nc;
+  } else {
+    const long long i0 = item % p.n0;
+    const long long rem = item / p.n0;
+    chunk = rem % nc;
+    s = i0 + p.n0 * (rem / nc);
+  }
+}
+
+template <typename R, int M>
+__global__ void __launch_bounds__(128) long_reduce_kernel(const BatchArgs<R> p, long long nc,
+                                                          R *__restrict__ ra, R *__restrict__ rb,
+                                                          R *__restrict__ rc,
+                                                          R *__restrict__ rd) {
+  const long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= p.nsys * nc) return;
+  long long s, chunk;
+  long_item(p, item, nc, s, chunk);
+  const long long base = sys_base(p, s);
+  const int row0 = (int)(chunk * M);
+  R a[M], b[M], c[M], d[M];
+  load_chunk<R, M, false>(p, base, row0, true, a, b, c, d);
+  bool bad = false;
+  chunk_forward<R, M>(a, b, c, d, bad);
+  chunk_backward<R, M>(a, c, d, bad);
+  const long long o = s * 2 * nc + 2 * chunk;
+  ra[o] = a[0];
+  rb[o] = R(1);
+  rc[o] = c[0];
+  rd[o] = d[0];
+  ra[o + 1] = a[M - 1];
+  rb[o + 1] = R(1);
+  rc[o + 1] = c[M - 1];
+  rd[o + 1] = d[M - 1];
+  report_bad_pivot(bad, p.flag);
+}
+
+template <typename R, int M, bool INC>
+__global__ void __launch_bounds__(128) long_substitute_kernel(const BatchArgs<R> p, long long nc,
+                                                              const R *__restrict__ xr) {
+  const long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= p.nsys * nc) return;
+  long long s, chunk;
+  long_item(p, item, nc, s, chunk);
+  const long long base = sys_base(p, s);
+  const int row0 = (int)(chunk * M);
+  R a[M], b[M], c[M], d[M];
+  load_chunk<R, M, false>(p, base, row0, true, a, b, c, d);
+  bool bad = false;
+  chunk_forward<R, M>(a, b, c, d, bad);
+  chunk_backward<R, M>(a, c, d, bad);
+  const long long o = s * 2 * nc + 2 * chunk;
+  chunk_substitute<R, M>(a, c, d, xr[o], xr[o + 1]);
+  store_chunk<R, M, INC, false>(p, base, row0, true, d);
+}
+
+}  // namespace trid
