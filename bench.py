@@ -172,7 +172,7 @@ def cpu_reference_rate(n, planes, steps, dtype, time_budget=10.0):
     step()
     one = time.perf_counter() - t0
     if steps <= 0:
-        steps = max(2, min(50, int(time_budget / max(one, 1e-6))))
+        steps = max(2, min(2000, int(time_budget / max(one, 1e-6))))
     t0 = time.perf_counter()
     for _ in range(steps):
         step()

@@ -54,9 +54,12 @@ def padded_index(dims, pads):
 
 
 def to_padded(x, dims, pads, fill=np.nan):
-    """Copy a compact x-fastest array into the interior of a padded one."""
-    full = np.full(int(np.prod(pads)), fill, dtype=x.dtype)
-    full[padded_index(dims, pads)] = x
+    """Copy a compact x-fastest array into the interior of a padded one (grown
+    past prod(pads) when a dimension has no padding to hold the offset)."""
+    idx = padded_index(dims, pads)
+    size = max(int(np.prod(pads)), int(idx.max()) + 1 if idx.size else 0)
+    full = np.full(size, fill, dtype=x.dtype)
+    full[idx] = x
     return full
 
 

@@ -87,7 +87,9 @@ def test_force_plan_round_trip():
     tb.force_plan(tb.FAMILY_PCR)
     assert tb.describe_plan(8, [20, 10], 0).startswith("pcr M=1 T=32")
     tb.force_plan(tb.FAMILY_LONG, 8)
-    assert tb.describe_plan(8, [20, 10], 0).startswith("long M=8")
+    assert tb.describe_plan(8, [100, 10], 0).startswith("long M=8")
+    # too short for the multi-block path: falls back to the hybrid
+    assert tb.describe_plan(8, [20, 10], 0).startswith("hybrid")
     tb.force_plan(tb.FAMILY_HYBRID, 4)
     assert tb.describe_plan(8, [20, 10], 0).startswith("hybrid M=4 T=8")
     tb.force_plan()

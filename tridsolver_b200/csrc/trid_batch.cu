@@ -46,16 +46,18 @@ static int default_m(int N) {
 }
 
 template <typename R>
-Plan choose_plan(const BatchArgs<R> &p, bool aligned16) {
+Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
   const Settings &st = settings();
   Plan plan;
   const int N = p.N;
-  int fam = st.force_family;
-  int M = st.force_m;
+  int fam = honour_force ? st.force_family : TRID_FAMILY_AUTO;
+  int M = honour_force ? st.force_m : 0;
   if (fam == TRID_FAMILY_AUTO) fam = N > warp_max_rows<R>() ? TRID_FAMILY_LONG : TRID_FAMILY_HYBRID;
   if (fam == TRID_FAMILY_PCR && N > 32) fam = TRID_FAMILY_HYBRID;
   if (fam == TRID_FAMILY_HYBRID && M == 0) M = default_m<R>(N);
   if (fam == TRID_FAMILY_HYBRID && (long long)M * 32 < N) fam = TRID_FAMILY_LONG, M = 0;
+  // the long path needs a reduced system (2 rows per chunk) shorter than N
+  if (fam == TRID_FAMILY_LONG && N <= 2 * 16) fam = TRID_FAMILY_HYBRID, M = default_m<R>(N);
   plan.family = fam;
   if (fam == TRID_FAMILY_PCR) {
     plan.M = 1;
@@ -135,6 +137,7 @@ static cudaError_t launch_pcr(const BatchArgs<R> &p, const Plan &plan, cudaStrea
 template <typename R, int M, bool INC>
 static cudaError_t launch_long_m(const BatchArgs<R> &p, cudaStream_t st) {
   const long long nc = ((long long)p.N + M - 1) / M;
+  if (2 * nc >= p.N) return cudaErrorInvalidValue;  // would not shrink
   const long long nred = p.nsys * 2 * nc;
   R *scratch = nullptr;
   cudaError_t e = cudaMallocAsync((void **)&scratch, (size_t)nred * 4 * sizeof(R), st);
@@ -161,7 +164,9 @@ static cudaError_t launch_long_m(const BatchArgs<R> &p, cudaStream_t st) {
     q.st1 = 0;
     q.stride = 1;
     q.flag = p.flag;
-    Plan qp = choose_plan<R>(q, vec_aligned<R>(q));
+    // the reduced batch always takes the automatic plan: a forced family
+    // applies to the caller's problem only
+    Plan qp = choose_plan<R>(q, vec_aligned<R>(q), false);
     e = launch_batch<R, false>(q, qp, st);
   }
   if (e == cudaSuccess) {
@@ -185,7 +190,7 @@ cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t s
 }
 
 #define INSTANTIATE(R)                                                                  \
-  template Plan choose_plan<R>(const BatchArgs<R> &, bool);                           \
+  template Plan choose_plan<R>(const BatchArgs<R> &, bool, bool);                           \
   template bool vec_aligned<R>(const BatchArgs<R> &);                                 \
   template cudaError_t launch_batch<R, false>(const BatchArgs<R> &, const Plan &,     \
                                               cudaStream_t);                          \

@@ -36,8 +36,10 @@ extern std::atomic<unsigned long long> g_launches;
 unsigned *pivot_flag_device();
 bool pivot_flag_take();  // reads and clears the word of the current device
 
+// honour_force: apply the calling thread's tridForcePlan setting (top-level
+// calls only; internal recursions use the automatic table).
 template <typename R>
-Plan choose_plan(const BatchArgs<R> &p, bool aligned16);
+Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force = true);
 
 // Enqueues the solve of batch p on `st` (no synchronisation).
 template <typename R, bool INC>
