@@ -49,6 +49,10 @@ EXTERN_C unsigned long long tridGetLaunchCount(void);
 #define TRID_FAMILY_LONG 2
 EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
 
+/* Pins the number of neighbouring systems one thread block of the strided
+ * hybrid handles (a power of two; 0 restores the automatic choice). */
+EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
+
 /* Describes the plan the next solve of this shape would use, e.g.
  * "hybrid M=16 T=32 W=1 vec" (for logs and tests). Returns the length. */
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,

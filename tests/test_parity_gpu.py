@@ -104,11 +104,15 @@ def test_golden_padded(name, dt):
 
 # ---- seeded batches against the oracle --------------------------------------------
 
-SHAPES = [([1], 0), ([2], 0), ([3], 0), ([31], 0), ([33], 0), ([200], 0), ([1000], 0),
+SHAPES = [([1], 0), ([2], 0), ([3], 0), ([31], 0), ([33], 0), ([200], 0), ([201], 0), ([1000], 0),
+          ([1023], 0), ([1, 1, 1000], 2),
           ([5, 3], 1), ([33, 31], 0), ([33, 31], 1), ([9, 10, 11], 0), ([9, 10, 11], 1),
           ([9, 10, 11], 2), ([64, 48, 40], 0), ([64, 48, 40], 1), ([64, 48, 40], 2),
           ([256, 16, 8], 0), ([7, 512, 3], 1), ([4, 3, 512], 2), ([1, 1, 700], 2),
-          ([511, 2, 2], 0), ([3, 257, 5], 1)]
+          ([511, 2, 2], 0), ([3, 257, 5], 1),
+          # strided: reduced rows per lane 2, 4 and 8, a partial group of
+          # systems, lengths that do not fill the chunks
+          ([50, 3, 200], 2), ([17, 700, 2], 1), ([33, 5, 400], 2), ([40, 130], 1)]
 
 
 def _check(dims, solvedim, dt, inc, oracle, reference, pads=None, offset=0, seed=0):

@@ -31,6 +31,7 @@ SYMBOLS = {
     "tridGetPivotStatus": (_I, []),
     "tridGetLaunchCount": (ctypes.c_ulonglong, []),
     "tridForcePlan": (_I, [_I, _I]),
+    "tridForceSystemsPerBlock": (_I, [_I]),
     "tridDescribePlan": (_I, [_I, _I, _I, _IP, _IP, ctypes.c_char_p, _I]),
 }
 

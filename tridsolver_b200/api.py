@@ -131,6 +131,12 @@ def force_plan(family=FAMILY_AUTO, rows_per_thread=0):
         raise TridError(st, "tridForcePlan")
 
 
+def force_systems_per_block(systems=0):
+    st = _lib.load().tridForceSystemsPerBlock(int(systems))
+    if st != 0:
+        raise TridError(st, "tridForceSystemsPerBlock")
+
+
 def describe_plan(dtype_bytes, dims, solvedim, pads=None):
     pads = dims if pads is None else pads
     buf = ctypes.create_string_buffer(128)

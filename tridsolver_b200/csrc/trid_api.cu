@@ -236,6 +236,12 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread) {
   return TRID_STATUS_SUCCESS;
 }
 
+EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems) {
+  if (systems < 0 || systems > 256 || (systems & (systems - 1))) return TRID_STATUS_INVALID_VALUE;
+  settings().force_w = systems;
+  return TRID_STATUS_SUCCESS;
+}
+
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
                               const int *pads, char *buf, int buflen) {
   std::string desc;

@@ -1,5 +1,6 @@
 // Plan selection and launchers of the batched solve kernels.
 #include <cstdio>
+#include <cstring>
 #include <string>
 
 #include "trid_internal.h"
@@ -11,7 +12,8 @@ std::atomic<unsigned long long> g_launches{0};
 std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
-  snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W, vec ? " vec" : "");
+  snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
+           smem ? " smem" : vec ? " vec" : "");
   return buf;
 }
 
@@ -31,18 +33,29 @@ bool vec_aligned(const BatchArgs<R> &p) {
   return true;
 }
 
-// Largest system the single-warp hybrid holds: 32 lanes x M_max rows, with
-// M_max = 16 (double) or 32 (float) so a lane's chunk state stays in
-// registers without spilling.
-template <typename R> constexpr int warp_max_rows() { return sizeof(R) == 8 ? 512 : 1024; }
+// Which hybrid shapes have kernels: contiguous batches keep a system inside
+// one warp (T <= 32); strided batches re-deal the reduced rows through shared
+// memory, so a system may span up to 128 chunks (KR = 2T/32 reduced rows per
+// lane, instantiated for the M listed here).
+static bool hybrid_supported(bool contig, int M, int T) {
+  if (T <= 32) return true;
+  if (contig) return false;
+  if (T == 64) return M == 4 || M == 8 || M == 16;
+  if (T == 128) return M == 4 || M == 8;
+  return false;
+}
 
-// Built-in table: rows per thread by system length (see DESIGN.md for the
-// measurements behind it).
+// Built-in table of rows per thread by system length and layout; the
+// autotuner can replace it per shape (see DESIGN.md for the measurements).
 template <typename R>
-static int default_m(int N) {
-  if (N <= 256) return 8;
-  if (N <= 512) return 16;
-  return 32;
+static int default_m(int N, bool contig) {
+  if (contig) {
+    if (N <= 256) return 8;
+    if (N <= 512) return 16;
+    return 32;
+  }
+  if (sizeof(R) == 8) return 8;
+  return N <= 256 ? 8 : 16;
 }
 
 template <typename R>
@@ -50,40 +63,69 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
   const Settings &st = settings();
   Plan plan;
   const int N = p.N;
+  const bool contig = p.stride == 1;
   int fam = honour_force ? st.force_family : TRID_FAMILY_AUTO;
   int M = honour_force ? st.force_m : 0;
-  if (fam == TRID_FAMILY_AUTO) fam = N > warp_max_rows<R>() ? TRID_FAMILY_LONG : TRID_FAMILY_HYBRID;
-  if (fam == TRID_FAMILY_PCR && N > 32) fam = TRID_FAMILY_HYBRID;
-  if (fam == TRID_FAMILY_HYBRID && M == 0) M = default_m<R>(N);
-  if (fam == TRID_FAMILY_HYBRID && (long long)M * 32 < N) fam = TRID_FAMILY_LONG, M = 0;
-  // the long path needs a reduced system (2 rows per chunk) shorter than N
-  if (fam == TRID_FAMILY_LONG && N <= 2 * 16) fam = TRID_FAMILY_HYBRID, M = default_m<R>(N);
-  plan.family = fam;
+  if (fam == TRID_FAMILY_PCR && N > 32) fam = TRID_FAMILY_HYBRID, M = 0;
   if (fam == TRID_FAMILY_PCR) {
+    plan.family = fam;
     plan.M = 1;
     plan.T = pow2_ceil(N < 1 ? 1 : N);
     return plan;
   }
-  if (fam == TRID_FAMILY_LONG) {
-    plan.M = (M == 8 || M == 16) ? M : 16;
-    return plan;
+  // the long path needs a reduced system (2 rows per chunk) shorter than N
+  if (fam == TRID_FAMILY_LONG && N <= 32) fam = TRID_FAMILY_HYBRID, M = 0;
+  if (fam != TRID_FAMILY_LONG) {
+    if (M == 0) M = default_m<R>(N, contig);
+    const int T = pow2_ceil((N + M - 1) / M);
+    if (hybrid_supported(contig, M, T) && (sizeof(R) == 4 || M <= 16 || contig == false)) {
+      plan.family = TRID_FAMILY_HYBRID;
+      plan.M = M;
+      plan.T = T;
+      if (contig) {
+        plan.vec = aligned16 && ((M * (int)sizeof(R)) % 16 == 0);
+        plan.smem = plan.vec && T == 32;
+      } else {
+        // at least 64 contiguous bytes per row: rows of a z solve are a whole
+        // plane apart, and z throughput grows with the bytes per row access
+        const int wseg = 64 / (int)sizeof(R);
+        int W = 256 / T > wseg ? 256 / T : wseg;
+        const int wmin = 32 / T > 1 ? 32 / T : 1;
+        const int n0p = pow2_ceil(p.n0);
+        if (W > n0p) W = n0p;
+        if (honour_force && st.force_w > 0) W = st.force_w;
+        if (W < wmin) W = wmin;
+        const int tmax = (T > 32 || M * (int)sizeof(R) <= 64) ? 512 : 256;
+        if (W * T > tmax) W = tmax / T;
+        plan.W = W;
+      }
+      return plan;
+    }
+    M = 0;
   }
-  plan.M = M;
-  plan.T = pow2_ceil((N + M - 1) / M);
-  if (p.stride == 1) {
-    plan.vec = aligned16 && ((M * (int)sizeof(R)) % 16 == 0);
-  } else {
-    int W = 256 / plan.T;
-    const int wmin = 32 / plan.T > 1 ? 32 / plan.T : 1;
-    const int n0p = pow2_ceil(p.n0);
-    if (W > n0p) W = n0p;
-    if (W < wmin) W = wmin;
-    plan.W = W;
-  }
+  plan.family = TRID_FAMILY_LONG;
+  plan.M = (M == 8 || M == 16) ? M : 16;
   return plan;
 }
 
 // ---------------------------------------------------------------------------
+
+template <typename K>
+static void allow_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename R, int M, int KR, bool INC>
+static cudaError_t launch_strided(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  const int threads = plan.W * plan.T;
+  const long long ngx = (p.n0 + plan.W - 1) / plan.W;
+  const long long n1 = p.nsys / p.n0;
+  const long long blocks = ngx * n1;
+  const size_t smem = (size_t)6 * plan.T * (plan.W + 1) * sizeof(R);
+  allow_smem(strided_kernel<R, M, KR, INC>, smem);
+  strided_kernel<R, M, KR, INC><<<(unsigned)blocks, threads, smem, st>>>(p, plan.T, plan.W, ngx);
+  return cudaSuccess;
+}
 
 template <typename R, int M, bool INC>
 static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
@@ -91,7 +133,16 @@ static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cuda
     const int threads = 128;
     const long long total = p.nsys * plan.T;
     const long long blocks = (total + threads - 1) / threads;
-    if (plan.vec) {
+    if (plan.smem) {
+      if constexpr ((M * sizeof(R)) % 16 == 0) {
+        using L = SmemLayout<R, M>;
+        const size_t smem = (size_t)(threads / 32) * (INC ? 5 : 4) * L::BUF * sizeof(R);
+        allow_smem(contig_smem_kernel<R, M, INC>, smem);
+        contig_smem_kernel<R, M, INC><<<(unsigned)blocks, threads, smem, st>>>(p);
+      } else {
+        return cudaErrorInvalidValue;
+      }
+    } else if (plan.vec) {
       if constexpr ((M * sizeof(R)) % 16 == 0) {
         contig_kernel<R, M, INC, true><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
       } else {
@@ -101,12 +152,15 @@ static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cuda
       contig_kernel<R, M, INC, false><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
     }
   } else {
-    const int threads = plan.W * plan.T;
-    const long long ngx = (p.n0 + plan.W - 1) / plan.W;
-    const long long n1 = p.nsys / p.n0;
-    const long long blocks = ngx * n1;
-    const size_t smem = (size_t)6 * plan.T * (plan.W + 1) * sizeof(R);
-    strided_kernel<R, M, INC><<<(unsigned)blocks, threads, smem, st>>>(p, plan.T, plan.W, ngx);
+    cudaError_t e = cudaErrorInvalidValue;
+    if (plan.T <= 32) {
+      e = launch_strided<R, M, 2, INC>(p, plan, st);
+    } else if (plan.T == 64) {
+      if constexpr (M == 4 || M == 8 || M == 16) e = launch_strided<R, M, 4, INC>(p, plan, st);
+    } else if (plan.T == 128) {
+      if constexpr (M == 4 || M == 8) e = launch_strided<R, M, 8, INC>(p, plan, st);
+    }
+    if (e != cudaSuccess) return e;
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();

@@ -226,6 +226,18 @@ __device__ __forceinline__ void report_bad_pivot(bool bad, unsigned *flag) {
   if (bad && flag) *reinterpret_cast<volatile unsigned *>(flag) = 1u;
 }
 
+// Asynchronous global -> shared copy of one 16-byte unit (cp.async, bypassing
+// registers and L1); `bytes` < 16 reads only that many bytes and zero-fills
+// the rest. Both addresses must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src, int bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem_src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // 16-byte vector types for contiguous rows.
 template <typename R> struct Vec16;
 template <> struct Vec16<double> {

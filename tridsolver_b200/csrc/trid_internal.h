@@ -17,6 +17,7 @@ struct Plan {
   int T = 1;                        // threads per system (hybrid, pcr)
   int W = 1;                        // systems per block (strided hybrid)
   bool vec = false;                 // 16-byte vector loads (contiguous hybrid)
+  bool smem = false;                // warp-per-system staging through shared memory
   std::string describe() const;
 };
 
@@ -26,6 +27,7 @@ struct Settings {
   bool blocking = true;
   int force_family = TRID_FAMILY_AUTO;
   int force_m = 0;
+  int force_w = 0;
 };
 Settings &settings();
 

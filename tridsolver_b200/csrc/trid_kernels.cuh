@@ -145,12 +145,154 @@ __global__ void __launch_bounds__(128) contig_kernel(const BatchArgs<R> p, int T
 }
 
 // ---------------------------------------------------------------------------
+// contig_smem_kernel: stride == 1, one warp per system (T = 32), 16-byte
+// aligned systems. The warp stages its system through shared memory: the
+// copies are coalesced 16-byte cp.async units (512 contiguous bytes per warp
+// instruction), and each lane then reads its own chunk row from a padded
+// layout (one spare 16-byte unit per chunk row, so the 16-byte reads of eight
+// neighbouring lanes hit eight different bank groups). The result goes back
+// the same way. Direct per-lane chunk loads instead make every warp load
+// touch 32 separate lines and saturate L1.
+template <typename R, int M> struct SmemLayout {
+  static constexpr int V = 16 / (int)sizeof(R);  // elements per 16-byte unit
+  static constexpr int ROW = M + V;              // padded chunk row, elements
+  static constexpr int BUF = 32 * ROW;           // one array of one system
+};
+
+template <typename R, int M>
+__device__ __forceinline__ void lds_row(const R *row, R (&v)[M]) {
+  using Vt = typename Vec16<R>::T;
+  constexpr int n = Vec16<R>::n;
+  const Vt *q = reinterpret_cast<const Vt *>(row);
+#pragma unroll
+  for (int i = 0; i < M / n; ++i) {
+    Vt x = q[i];
+    if constexpr (n == 2) {
+      v[2 * i] = x.x;
+      v[2 * i + 1] = x.y;
+    } else {
+      v[4 * i] = x.x;
+      v[4 * i + 1] = x.y;
+      v[4 * i + 2] = x.z;
+      v[4 * i + 3] = x.w;
+    }
+  }
+}
+
+template <typename R, int M, bool INC>
+__global__ void __launch_bounds__(128) contig_smem_kernel(const BatchArgs<R> p) {
+  using L = SmemLayout<R, M>;
+  using Vt = typename Vec16<R>::T;
+  constexpr int V = L::V;
+  constexpr int NA = INC ? 5 : 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *buf = reinterpret_cast<R *>(smem_raw) + (threadIdx.x >> 5) * (NA * L::BUF);
+  const int lane = threadIdx.x & 31;
+  const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (s >= p.nsys) return;  // uniform per warp
+  const long long base = sys_base(p, s);
+  const int N = p.N;
+  const int nunits = (N + V - 1) / V;
+  const R *src[5] = {p.a + base, p.b + base, p.c + base, p.d_in + base,
+                     INC ? p.u + base : p.d_in + base};
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    for (int un = lane; un < nunits; un += 32) {
+      const int e = un * V;
+      const int left = N - e;
+      cp_async16(buf + k * L::BUF + e + (e / M) * V, src[k] + e,
+                 (left >= V ? V : left) * (int)sizeof(R));
+    }
+  }
+  cp_async_wait_all();
+  __syncwarp();
+
+  const int row0 = lane * M;
+  R ra[M], rb[M], rc[M], rd[M];
+  lds_row<R, M>(buf + 0 * L::BUF + lane * L::ROW, ra);
+  lds_row<R, M>(buf + 1 * L::BUF + lane * L::ROW, rb);
+  lds_row<R, M>(buf + 2 * L::BUF + lane * L::ROW, rc);
+  lds_row<R, M>(buf + 3 * L::BUF + lane * L::ROW, rd);
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int row = row0 + i;
+    if (row >= N) {
+      ra[i] = R(0);
+      rb[i] = R(1);
+      rc[i] = R(0);
+      rd[i] = R(0);
+    }
+    if (row == N - 1) rc[i] = R(0);
+  }
+  if (lane == 0) ra[0] = R(0);
+  bool bad = false;
+  chunk_forward<R, M>(ra, rb, rc, rd, bad);
+  chunk_backward<R, M>(ra, rc, rd, bad);
+  Row<R> top{ra[0], rc[0], rd[0]};
+  Row<R> bot{ra[M - 1], rc[M - 1], rd[M - 1]};
+  R y, z;
+  reduced_solve<R>(top, bot, lane, 32, y, z, bad);
+  chunk_substitute<R, M>(ra, rc, rd, y, z);
+  // each lane overwrites only its own row of the `a` buffer
+  {
+    Vt *q = reinterpret_cast<Vt *>(buf + lane * L::ROW);
+#pragma unroll
+    for (int i = 0; i < M / V; ++i) {
+      Vt x;
+      if constexpr (V == 2) {
+        x.x = rd[2 * i];
+        x.y = rd[2 * i + 1];
+      } else {
+        x.x = rd[4 * i];
+        x.y = rd[4 * i + 1];
+        x.z = rd[4 * i + 2];
+        x.w = rd[4 * i + 3];
+      }
+      q[i] = x;
+    }
+  }
+  __syncwarp();
+  R *dst = INC ? p.u + base : p.d_out + base;
+  for (int un = lane; un < nunits; un += 32) {
+    const int e = un * V;
+    const int idx = e + (e / M) * V;
+    Vt x = *reinterpret_cast<const Vt *>(buf + idx);
+    if (INC) {
+      const Vt uo = *reinterpret_cast<const Vt *>(buf + 4 * L::BUF + idx);
+      if constexpr (V == 2) {
+        x.x += uo.x;
+        x.y += uo.y;
+      } else {
+        x.x += uo.x;
+        x.y += uo.y;
+        x.z += uo.z;
+        x.w += uo.w;
+      }
+    }
+    if (e + V <= N) {
+      *reinterpret_cast<Vt *>(dst + e) = x;
+    } else {
+      const R *xs = reinterpret_cast<const R *>(&x);
+      for (int i = 0; i < N - e; ++i) dst[e + i] = xs[i];
+    }
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+// ---------------------------------------------------------------------------
 // strided_kernel: block = W systems (neighbouring i0) x T chunks, thread
 // (s, t) = (tid % W, tid / W). W*T is a multiple of 32.
-template <typename R, int M, bool INC>
-__global__ void __launch_bounds__(256) strided_kernel(const BatchArgs<R> p, int T, int W,
-                                                      long long ngx) {
-  extern __shared__ unsigned char smem_raw[];
+// After chunk elimination the reduced rows go to shared memory, slot (t, s),
+// and are dealt again so that one system's 2T reduced rows sit in one warp:
+//   KR == 2 (T <= 32): T consecutive lanes, two rows (top, bottom) each, solved
+//                      by reduced_solve over a T-lane segment;
+//   KR >= 4 (T = 16*KR): one warp per system, KR consecutive reduced rows per
+//                      lane, eliminated locally as a chunk of KR rows before
+//                      the 32-lane reduced_solve.
+template <typename R, int M, int KR, bool INC>
+__global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
+    strided_kernel(const BatchArgs<R> p, int T, int W, long long ngx) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   R *sm = reinterpret_cast<R *>(smem_raw);
   const int tid = threadIdx.x;
   const int s = tid % W;
@@ -167,7 +309,7 @@ __global__ void __launch_bounds__(256) strided_kernel(const BatchArgs<R> p, int 
   chunk_forward<R, M>(ra, rb, rc, rd, bad);
   chunk_backward<R, M>(ra, rc, rd, bad);
 
-  // re-deal the reduced rows: slot (t, s) at t*(W+1)+s, six values each
+  // slot (t, s) at t*(W+1)+s, six values each
   const int ld = W + 1;
   const int nslot = T * ld;
   {
@@ -180,7 +322,7 @@ __global__ void __launch_bounds__(256) strided_kernel(const BatchArgs<R> p, int 
     sm[5 * nslot + k] = rd[M - 1];
   }
   __syncthreads();
-  {
+  if constexpr (KR == 2) {
     const int s2 = tid / T;
     const int t2 = tid & (T - 1);
     const int k = t2 * ld + s2;
@@ -191,6 +333,37 @@ __global__ void __launch_bounds__(256) strided_kernel(const BatchArgs<R> p, int 
     // slot k is read and rewritten by this thread only
     sm[0 * nslot + k] = y;
     sm[1 * nslot + k] = z;
+  } else {
+    const int w = tid >> 5;
+    const int l = tid & 31;
+    if (w < W) {  // warp w solves the reduced system of system w
+      R qa[KR], qb[KR], qc[KR], qd[KR];
+#pragma unroll
+      for (int j = 0; j < KR / 2; ++j) {
+        const int k = (l * (KR / 2) + j) * ld + w;
+        qa[2 * j] = sm[0 * nslot + k];
+        qc[2 * j] = sm[1 * nslot + k];
+        qd[2 * j] = sm[2 * nslot + k];
+        qa[2 * j + 1] = sm[3 * nslot + k];
+        qc[2 * j + 1] = sm[4 * nslot + k];
+        qd[2 * j + 1] = sm[5 * nslot + k];
+        qb[2 * j] = R(1);
+        qb[2 * j + 1] = R(1);
+      }
+      chunk_forward<R, KR>(qa, qb, qc, qd, bad);
+      chunk_backward<R, KR>(qa, qc, qd, bad);
+      Row<R> top{qa[0], qc[0], qd[0]};
+      Row<R> bot{qa[KR - 1], qc[KR - 1], qd[KR - 1]};
+      R y, z;
+      reduced_solve<R>(top, bot, l, 32, y, z, bad);
+      chunk_substitute<R, KR>(qa, qc, qd, y, z);
+#pragma unroll
+      for (int j = 0; j < KR / 2; ++j) {
+        const int k = (l * (KR / 2) + j) * ld + w;
+        sm[0 * nslot + k] = qd[2 * j];
+        sm[1 * nslot + k] = qd[2 * j + 1];
+      }
+    }
   }
   __syncthreads();
   const int k = t * ld + s;
