@@ -53,6 +53,26 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
 
+/* ---- solve without allocating ------------------------------------------
+ * No counterpart in the reference. tridDmtsvStridedBatch with the same
+ * arguments and results, for callers that cannot allocate device memory
+ * (services that reserve and account for all device memory up front,
+ * real-time loops where an allocation's latency or failure is not
+ * acceptable): the regular entry point allocates scratch for systems longer
+ * than one warp holds and pins a host word on first use; this one allocates
+ * nothing. Its scratch is one fixed 16 MiB array in device memory that every
+ * GPU loading the library holds until exit. Problems whose long-system
+ * scratch would exceed it return TRID_STATUS_INVALID_VALUE (with a message on
+ * stderr); systems short enough for one warp per system (N <= 512 along x,
+ * N <= 1024 along y or z) need none. All calls share the array, so calls that
+ * overlap on the GPU race; the first call on a device looks up the array's
+ * address and should come before any stream capture. Zero pivots are
+ * reported in blocking mode only. */
+EXTERN_C tridStatus_t tridDmtsvStridedBatchNoAlloc(const TridParams *ctx, const double *a,
+                                                   const double *b, const double *c, double *d,
+                                                   int ndim, int solvedim, const int *dims,
+                                                   const int *pads);
+
 /* Describes the plan the next solve of this shape would use, e.g.
  * "hybrid M=16 T=32 W=1 vec" (for logs and tests). Returns the length. */
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
