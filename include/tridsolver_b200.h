@@ -53,6 +53,23 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
 
+/* ---- FP32 storage, FP64 accuracy -----------------------------------------
+ * No counterpart in the reference. Solves T x = d where a, b, c are stored in
+ * FP32 (the system is exactly those values, promoted to FP64) and d is FP64;
+ * x overwrites d. The solve runs in FP32; only the residual r = d - T x and
+ * the accumulation x += dx run in FP64, repeated on chip until
+ * max|dx| <= tol * max|x| for every system or max_iters FP32 solves. One pass
+ * over memory: 28 bytes per element against 40 for tridDmtsvStridedBatch.
+ * Blocking calls report the largest iteration count and the largest final
+ * relative correction over all systems in *iters_out / *correction_out (-1
+ * when not blocking). Supports N <= 512 (longer systems return
+ * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
+EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const float *a,
+                                                 const float *b, const float *c, double *d,
+                                                 int ndim, int solvedim, const int *dims,
+                                                 const int *pads, int max_iters, double tol,
+                                                 int *iters_out, double *correction_out);
+
 /* ---- solve without allocating ------------------------------------------
  * No counterpart in the reference. tridDmtsvStridedBatch with the same
  * arguments and results, for callers that cannot allocate device memory

@@ -7,8 +7,8 @@ def make_system(dims, solvedim, dtype=np.float64, seed=0, margin=None):
     """Seeded batch in the reference layout (flat, x fastest).
 
     a, c ~ U(-0.5, 0.5) with a = 0 on the first and c = 0 on the last row of
-    every system along `solvedim`; b = 1 + |a| + |c| + U(0, 1) (or + margin
-    when given, an array/scalar of diagonal-dominance margins); d ~ N(0, 1).
+    every system along `solvedim`; b = 1 + |a| + |c| + U(0, 1), or, when
+    `margin` (array or scalar) is given, b = |a| + |c| + margin; d ~ N(0, 1).
     """
     rng = np.random.default_rng(seed)
     shape = tuple(reversed(dims))  # C-order view: x is the last axis
@@ -21,8 +21,10 @@ def make_system(dims, solvedim, dtype=np.float64, seed=0, margin=None):
     idxl = [slice(None)] * len(dims)
     idxl[ax] = -1
     c[tuple(idxl)] = 0.0
-    extra = rng.uniform(0.0, 1.0, shape) if margin is None else margin
-    b = 1.0 + np.abs(a) + np.abs(c) + extra
+    if margin is None:
+        b = 1.0 + np.abs(a) + np.abs(c) + rng.uniform(0.0, 1.0, shape)
+    else:  # diagonal-dominance margin b - |a| - |c|
+        b = np.abs(a) + np.abs(c) + margin
     d = rng.standard_normal(shape)
     out = [np.ascontiguousarray(v.reshape(-1), dtype=dtype) for v in (a, b, c, d)]
     return out

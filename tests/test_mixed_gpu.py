@@ -1,0 +1,63 @@
+"""GPU: FP32-storage solve with FP64 refinement (tridDmtsvStridedBatchMixed).
+
+The system is the FP32-stored coefficients taken exactly, so the FP64 oracle
+(oracle/trid_oracle.c, the reference's Thomas recurrence) on the promoted
+coefficients is the exact answer to match: normwise relative error <= 1e-12,
+as for the plain FP64 path, across diagonal-dominance margins from 1e-3 to 1
+(the precision configuration's range) and along x, y and z.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import tridsolver_b200 as tb
+from helpers import make_system, normwise
+from oracle.pyoracle import Restatement
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Restatement()
+
+
+def _problem(dims, solvedim, margin, seed):
+    rng = np.random.default_rng(seed)
+    shape = tuple(reversed(dims))
+    marg = 10.0 ** rng.uniform(np.log10(margin), 0.0, shape) if margin < 1 else np.ones(shape)
+    a, b, c, d = make_system(dims, solvedim, np.float64, seed=seed, margin=marg.reshape(shape))
+    a32, b32, c32 = (v.astype(np.float32) for v in (a, b, c))
+    return a32, b32, c32, d
+
+
+SHAPES = [([512, 4, 3], 0), ([256, 8, 2], 0), ([200, 7], 0), ([33, 3], 0), ([1], 0),
+          ([16, 512, 2], 1), ([10, 300], 1), ([24, 3, 512], 2), ([40, 5, 256], 2), ([9, 2, 7], 2)]
+
+
+@pytest.mark.parametrize("margin", [1e-3, 1e-1, 1.0])
+@pytest.mark.parametrize("dims,solvedim", SHAPES)
+def test_mixed_matches_fp64_oracle(dims, solvedim, margin, oracle):
+    a32, b32, c32, d = _problem(dims, solvedim, margin, seed=sum(dims) + solvedim)
+    want = d.copy()
+    oracle.strided_batch(*(v.astype(np.float64) for v in (a32, b32, c32)), want, dims, solvedim)
+    ta, tb_, tc = (torch.from_numpy(v).cuda() for v in (a32, b32, c32))
+    td = torch.from_numpy(d).cuda()
+    st, iters, corr = tb.tridDmtsvStridedBatchMixed(None, ta, tb_, tc, td, len(dims), solvedim,
+                                                    dims, dims, max_iters=12, tol=1e-13)
+    assert st == 0
+    assert 1 <= iters <= 12
+    err = normwise(td.cpu().numpy(), want)
+    assert err <= 1e-12, (err, iters, corr)
+
+
+def test_mixed_unsupported_cases_are_reported():
+    a32, b32, c32, d = _problem([600, 2], 0, 1.0, seed=1)
+    ta, tb_, tc = (torch.from_numpy(v).cuda() for v in (a32, b32, c32))
+    td = torch.from_numpy(d).cuda()
+    st, _, _ = tb.tridDmtsvStridedBatchMixed(None, ta, tb_, tc, td, 2, 0, [600, 2], [600, 2])
+    assert st == tb.TridStatus.MATRIX_TYPE_NOT_SUPPORTED
+    st, _, _ = tb.tridDmtsvStridedBatchMixed(None, ta, tb_, tc, td, 2, 0, [600, 2], [600, 2],
+                                             max_iters=0)
+    assert st == tb.TridStatus.INVALID_VALUE

@@ -33,6 +33,8 @@ SYMBOLS = {
     "tridForcePlan": (_I, [_I, _I]),
     "tridForceSystemsPerBlock": (_I, [_I]),
     "tridDescribePlan": (_I, [_I, _I, _I, _IP, _IP, ctypes.c_char_p, _I]),
+    "tridDmtsvStridedBatchMixed": (_I, [_P, _P, _P, _P, _P, _I, _I, _IP, _IP, _I, ctypes.c_double,
+                                        _IP, ctypes.POINTER(ctypes.c_double)]),
 }
 
 _lib = None

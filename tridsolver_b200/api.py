@@ -101,6 +101,20 @@ def tridSmtsvStridedBatchInc(ctx, a, b, c, d, u, ndim, solvedim, dims, pads):
                                                 _ints(pads))
 
 
+def tridDmtsvStridedBatchMixed(ctx, a, b, c, d, ndim, solvedim, dims, pads, max_iters=10,
+                               tol=1e-12):
+    """FP32-stored a, b, c; FP64 d (x overwrites it); FP32 solves refined in
+    FP64 on chip (include/tridsolver_b200.h). Returns (status, iterations,
+    final relative correction); the last two are -1 unless blocking."""
+    it = ctypes.c_int(-1)
+    corr = ctypes.c_double(-1.0)
+    st = _lib.load().tridDmtsvStridedBatchMixed(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                                int(ndim), int(solvedim), _ints(dims), _ints(pads),
+                                                int(max_iters), float(tol), ctypes.byref(it),
+                                                ctypes.byref(corr))
+    return st, it.value, corr.value
+
+
 # ---- execution control -------------------------------------------------------
 
 def set_stream(stream):

@@ -40,6 +40,9 @@ bool pivot_flag_take();  // reads and clears the word of the current device
 
 // honour_force: apply the calling thread's tridForcePlan setting (top-level
 // calls only; internal recursions use the automatic table).
+// CUDA error -> library status (trid_api.cu).
+tridStatus_t status_of(cudaError_t e);
+
 template <typename R>
 Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force = true);
 

@@ -280,59 +280,46 @@ __global__ void __launch_bounds__(128) contig_smem_kernel(const BatchArgs<R> p) 
 }
 
 // ---------------------------------------------------------------------------
-// strided_kernel: block = W systems (neighbouring i0) x T chunks, thread
-// (s, t) = (tid % W, tid / W). W*T is a multiple of 32.
-// After chunk elimination the reduced rows go to shared memory, slot (t, s),
-// and are dealt again so that one system's 2T reduced rows sit in one warp:
+// Block-level reduced solve for W systems x T chunks, thread (s, t) =
+// (tid % W, tid / W). The reduced rows go to shared memory, slot (t, s) at
+// t*(W+1)+s, and are dealt again so that one system's 2T reduced rows sit in
+// one warp:
 //   KR == 2 (T <= 32): T consecutive lanes, two rows (top, bottom) each, solved
 //                      by reduced_solve over a T-lane segment;
 //   KR >= 4 (T = 16*KR): one warp per system, KR consecutive reduced rows per
 //                      lane, eliminated locally as a chunk of KR rows before
 //                      the 32-lane reduced_solve.
-template <typename R, int M, int KR, bool INC>
-__global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
-    strided_kernel(const BatchArgs<R> p, int T, int W, long long ngx) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *sm = reinterpret_cast<R *>(smem_raw);
+// Returns the first (y) and last (z) unknown of the thread's chunk. `sm` holds
+// 6*T*(W+1) values; every thread of the block must call this.
+template <typename R, int KR>
+__device__ __forceinline__ void block_reduced_solve(R *sm, const Row<R> &top, const Row<R> &bot,
+                                                    int s, int t, int T, int W, R &y, R &z,
+                                                    bool &bad) {
   const int tid = threadIdx.x;
-  const int s = tid % W;
-  const int t = tid / W;
-  const long long gx = blockIdx.x % ngx;
-  const long long i1 = blockIdx.x / ngx;
-  const long long i0 = gx * W + s;
-  const bool active = i0 < p.n0;
-  const long long base = i0 * p.st0 + i1 * p.st1;
-  const int row0 = t * M;
-  R ra[M], rb[M], rc[M], rd[M];
-  load_chunk<R, M, false>(p, base, row0, active, ra, rb, rc, rd);
-  bool bad = false;
-  chunk_forward<R, M>(ra, rb, rc, rd, bad);
-  chunk_backward<R, M>(ra, rc, rd, bad);
-
-  // slot (t, s) at t*(W+1)+s, six values each
   const int ld = W + 1;
   const int nslot = T * ld;
+  __syncthreads();  // the previous use of sm is over
   {
     const int k = t * ld + s;
-    sm[0 * nslot + k] = ra[0];
-    sm[1 * nslot + k] = rc[0];
-    sm[2 * nslot + k] = rd[0];
-    sm[3 * nslot + k] = ra[M - 1];
-    sm[4 * nslot + k] = rc[M - 1];
-    sm[5 * nslot + k] = rd[M - 1];
+    sm[0 * nslot + k] = top.A;
+    sm[1 * nslot + k] = top.C;
+    sm[2 * nslot + k] = top.D;
+    sm[3 * nslot + k] = bot.A;
+    sm[4 * nslot + k] = bot.C;
+    sm[5 * nslot + k] = bot.D;
   }
   __syncthreads();
   if constexpr (KR == 2) {
     const int s2 = tid / T;
     const int t2 = tid & (T - 1);
     const int k = t2 * ld + s2;
-    Row<R> top{sm[0 * nslot + k], sm[1 * nslot + k], sm[2 * nslot + k]};
-    Row<R> bot{sm[3 * nslot + k], sm[4 * nslot + k], sm[5 * nslot + k]};
-    R y, z;
-    reduced_solve<R>(top, bot, t2, T, y, z, bad);
+    Row<R> tp{sm[0 * nslot + k], sm[1 * nslot + k], sm[2 * nslot + k]};
+    Row<R> bt{sm[3 * nslot + k], sm[4 * nslot + k], sm[5 * nslot + k]};
+    R yy, zz;
+    reduced_solve<R>(tp, bt, t2, T, yy, zz, bad);
     // slot k is read and rewritten by this thread only
-    sm[0 * nslot + k] = y;
-    sm[1 * nslot + k] = z;
+    sm[0 * nslot + k] = yy;
+    sm[1 * nslot + k] = zz;
   } else {
     const int w = tid >> 5;
     const int l = tid & 31;
@@ -352,11 +339,11 @@ __global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
       }
       chunk_forward<R, KR>(qa, qb, qc, qd, bad);
       chunk_backward<R, KR>(qa, qc, qd, bad);
-      Row<R> top{qa[0], qc[0], qd[0]};
-      Row<R> bot{qa[KR - 1], qc[KR - 1], qd[KR - 1]};
-      R y, z;
-      reduced_solve<R>(top, bot, l, 32, y, z, bad);
-      chunk_substitute<R, KR>(qa, qc, qd, y, z);
+      Row<R> tp{qa[0], qc[0], qd[0]};
+      Row<R> bt{qa[KR - 1], qc[KR - 1], qd[KR - 1]};
+      R yy, zz;
+      reduced_solve<R>(tp, bt, l, 32, yy, zz, bad);
+      chunk_substitute<R, KR>(qa, qc, qd, yy, zz);
 #pragma unroll
       for (int j = 0; j < KR / 2; ++j) {
         const int k = (l * (KR / 2) + j) * ld + w;
@@ -367,8 +354,35 @@ __global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
   }
   __syncthreads();
   const int k = t * ld + s;
-  const R y = sm[0 * nslot + k];
-  const R z = sm[1 * nslot + k];
+  y = sm[0 * nslot + k];
+  z = sm[1 * nslot + k];
+}
+
+// ---------------------------------------------------------------------------
+// strided_kernel: block = W systems (neighbouring i0) x T chunks, thread
+// (s, t) = (tid % W, tid / W). W*T is a multiple of 32.
+template <typename R, int M, int KR, bool INC>
+__global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
+    strided_kernel(const BatchArgs<R> p, int T, int W, long long ngx) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sm = reinterpret_cast<R *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int s = tid % W;
+  const int t = tid / W;
+  const long long gx = blockIdx.x % ngx;
+  const long long i1 = blockIdx.x / ngx;
+  const long long i0 = gx * W + s;
+  const bool active = i0 < p.n0;
+  const long long base = i0 * p.st0 + i1 * p.st1;
+  const int row0 = t * M;
+  R ra[M], rb[M], rc[M], rd[M];
+  load_chunk<R, M, false>(p, base, row0, active, ra, rb, rc, rd);
+  bool bad = false;
+  chunk_forward<R, M>(ra, rb, rc, rd, bad);
+  chunk_backward<R, M>(ra, rc, rd, bad);
+  R y, z;
+  block_reduced_solve<R, KR>(sm, Row<R>{ra[0], rc[0], rd[0]}, Row<R>{ra[M - 1], rc[M - 1], rd[M - 1]},
+                             s, t, T, W, y, z, bad);
   chunk_substitute<R, M>(ra, rc, rd, y, z);
   store_chunk<R, M, INC, false>(p, base, row0, active, rd);
   report_bad_pivot(bad && active, p.flag);
