@@ -53,6 +53,45 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
 
+/* ---- ADI heat-diffusion timestep -----------------------------------------
+ * No single counterpart in the reference: one timestep of its ADI
+ * application (apps/adi/src/adi_cuda.cu:282-326, preproc.cu:40-90) on an
+ * nx*ny*nz grid of device arrays (x fastest, no padding):
+ *   du = lambda*(sum of 6 neighbours - 6u) inside, 0 on the boundary;
+ *   a = c = -alpha*lambda, b = 1 + 2*alpha*lambda inside, identity rows on
+ *   the boundary (alpha = 1: a = c = -lambda, b = 1 + 2*lambda; alpha = 0.5:
+ *   the reference application's coefficients);
+ *   du <- x solve; du <- y solve; u += z solve.
+ * lambda = lam[*step] read on the device (lam[0] when step is NULL), and
+ * *step += 1 at the end, so one captured CUDA graph of a timestep replays a
+ * sequence of per-step lambdas. a, b, c, du are caller scratch of nx*ny*nz. */
+EXTERN_C tridStatus_t tridDADIStep(double *u, double *du, double *a, double *b, double *c,
+                                   const double *lam, int *step, double alpha, int nx, int ny,
+                                   int nz);
+EXTERN_C tridStatus_t tridSADIStep(float *u, float *du, float *a, float *b, float *c,
+                                   const float *lam, int *step, float alpha, int nx, int ny,
+                                   int nz);
+
+/* ---- adjoint ------------------------------------------------------------
+ * No counterpart in the reference. For x = T^{-1} d solved along `solvedim`
+ * (the forward call's arguments) and w = dL/dx, writes
+ *   dbar = T^{-T} w,  abar_i = -dbar_i x_{i-1},  bbar_i = -dbar_i x_i,
+ *   cbar_i = -dbar_i x_{i+1}   (abar = 0 on the first, cbar on the last row).
+ * abar, bbar, cbar may each be NULL (x is then not read if all three are);
+ * dbar may alias w. One pass, systems up to N = 1024 (longer ones return
+ * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). Layout rules as tridDmtsvStridedBatch. */
+EXTERN_C tridStatus_t tridDmtsvStridedBatchAdjoint(const TridParams *ctx, const double *a,
+                                                   const double *b, const double *c,
+                                                   const double *x, const double *w, double *dbar,
+                                                   double *abar, double *bbar, double *cbar,
+                                                   int ndim, int solvedim, const int *dims,
+                                                   const int *pads);
+EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const TridParams *ctx, const float *a,
+                                                   const float *b, const float *c, const float *x,
+                                                   const float *w, float *dbar, float *abar,
+                                                   float *bbar, float *cbar, int ndim,
+                                                   int solvedim, const int *dims, const int *pads);
+
 /* ---- FP32 storage, FP64 accuracy -----------------------------------------
  * No counterpart in the reference. Solves T x = d where a, b, c are stored in
  * FP32 (the system is exactly those values, promoted to FP64) and d is FP64;

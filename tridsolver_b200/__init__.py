@@ -9,5 +9,6 @@ from .api import (  # noqa: F401
     FAMILY_AUTO, FAMILY_HYBRID, FAMILY_LONG, FAMILY_PCR, TridError, TridParams, TridStatus,
     describe_plan, force_plan, force_systems_per_block, get_blocking, launch_count, on_stream, pivot_status,
     set_blocking, set_stream, solve, strided_batch, tridDmtsvStridedBatch,
-    tridDmtsvStridedBatchInc, tridDmtsvStridedBatchMixed, tridSmtsvStridedBatch, tridSmtsvStridedBatchInc)
+    tridDmtsvStridedBatchAdjoint, tridDmtsvStridedBatchInc, tridDmtsvStridedBatchMixed,
+    tridSmtsvStridedBatch, tridSmtsvStridedBatchAdjoint, tridSmtsvStridedBatchInc)
 from ._lib import LIB_PATH, load as load_library  # noqa: F401

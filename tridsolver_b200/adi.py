@@ -1,0 +1,142 @@
+"""ADI heat diffusion on the batched tridiagonal solver.
+
+Two forms of the reference application's timestep (apps/adi/src/adi_cuda.cu:
+282-326): RHS du = lambda * (7-point Laplacian of u) inside, identity rows and
+du = 0 on the Dirichlet boundary, then du <- x solve, du <- y solve,
+u += z solve, with a = c = -alpha*lambda, b = 1 + 2*alpha*lambda.
+
+* ``ADIHeat``: the native timestep (tridDADIStep / tridSADIStep, one
+  preprocessing kernel and three solves), with per-step lambdas read on the
+  device and an optional CUDA graph of one timestep replayed per step.
+* ``adi_step`` / ``adi_run``: the same timestep written with torch ops and
+  the differentiable solve (tridsolver_b200.autograd), so a multi-step run
+  backpropagates to the initial field and to every step's lambda;
+  ``adi_run`` recomputes segments of ``checkpoint_every`` steps in the
+  backward pass instead of storing every intermediate field.
+
+Tensors are (nz, ny, nx), C-contiguous: x is the fastest dimension as in the
+reference.
+"""
+
+import ctypes
+
+import torch
+import torch.utils.checkpoint
+
+from . import _lib, api
+from .autograd import trid_solve
+
+
+class ADIHeat:
+    """Native ADI timesteps on a field u (nz, ny, nx) of float32 or float64."""
+
+    def __init__(self, u, lams, alpha=1.0):
+        if u.dim() != 3 or not u.is_cuda or not u.is_contiguous():
+            raise ValueError("u: contiguous CUDA tensor (nz, ny, nx)")
+        self.u = u
+        self.nz, self.ny, self.nx = u.shape
+        self.du = torch.empty_like(u)
+        self.a = torch.empty_like(u)
+        self.b = torch.empty_like(u)
+        self.c = torch.empty_like(u)
+        self.lams = torch.as_tensor(lams, dtype=u.dtype, device=u.device).contiguous()
+        self.step_counter = torch.zeros(1, dtype=torch.int32, device=u.device)
+        self.alpha = alpha
+        self.graph = None
+        lib = _lib.load()
+        self._fn = lib.tridDADIStep if u.dtype == torch.float64 else lib.tridSADIStep
+        self._ctype = ctypes.c_double if u.dtype == torch.float64 else ctypes.c_float
+
+    def _launch(self):
+        st = self._fn(self.u.data_ptr(), self.du.data_ptr(), self.a.data_ptr(), self.b.data_ptr(),
+                      self.c.data_ptr(), self.lams.data_ptr(), self.step_counter.data_ptr(),
+                      self._ctype(self.alpha), self.nx, self.ny, self.nz)
+        if st != 0:
+            raise api.TridError(st, "ADI step")
+
+    def step(self):
+        """One timestep with lambda = lams[step], enqueued on the current stream."""
+        with torch.cuda.device(self.u.device), api.on_stream(blocking=False):
+            self._launch()
+
+    def capture(self):
+        """Capture one timestep into a CUDA graph (after one eager warm-up step,
+        which the caller's step counter includes)."""
+        self.step()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                with api.on_stream(s, blocking=False):
+                    self._launch()
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+        return g
+
+    def run(self, steps):
+        """`steps` timesteps: graph replays when captured, else eager launches."""
+        for _ in range(steps):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self.step()
+
+    def reset_counter(self, value=0):
+        self.step_counter.fill_(value)
+
+
+# ---- differentiable form --------------------------------------------------
+
+_masks = {}
+
+
+def _interior(shape, dtype, device):
+    key = (tuple(shape), dtype, device)
+    m = _masks.get(key)
+    if m is None:
+        m = torch.zeros(shape, dtype=dtype, device=device)
+        m[1:-1, 1:-1, 1:-1] = 1
+        _masks[key] = m
+    return m
+
+
+def adi_rhs(u, lam):
+    """lambda * (sum of the 6 neighbours - 6 u) inside, 0 on the boundary."""
+    lap = torch.zeros_like(u)
+    lap[1:-1, 1:-1, 1:-1] = (u[:-2, 1:-1, 1:-1] + u[2:, 1:-1, 1:-1] + u[1:-1, :-2, 1:-1] +
+                             u[1:-1, 2:, 1:-1] + u[1:-1, 1:-1, :-2] + u[1:-1, 1:-1, 2:] -
+                             6 * u[1:-1, 1:-1, 1:-1])
+    return lam * lap
+
+
+def adi_step(u, lam, alpha=1.0):
+    """One differentiable ADI timestep; lam is a 0-d tensor (may require grad)."""
+    m = _interior(u.shape, u.dtype, u.device)
+    a = -alpha * lam * m
+    b = 1 + 2 * alpha * lam * m
+    du = adi_rhs(u, lam)
+    du = trid_solve(a, b, a, du, dim=2)   # x
+    du = trid_solve(a, b, a, du, dim=1)   # y
+    return u + trid_solve(a, b, a, du, dim=0)  # z, added into u
+
+
+def _segment(u, lams, alpha):
+    for k in range(lams.shape[0]):
+        u = adi_step(u, lams[k], alpha)
+    return u
+
+
+def adi_run(u0, lams, alpha=1.0, checkpoint_every=10):
+    """len(lams) timesteps from u0; with checkpoint_every > 0 only every
+    k-th field is kept for the backward pass and segments are recomputed."""
+    u = u0
+    n = lams.shape[0]
+    for s0 in range(0, n, checkpoint_every if checkpoint_every > 0 else n):
+        seg = lams[s0:s0 + (checkpoint_every if checkpoint_every > 0 else n)]
+        if checkpoint_every > 0 and torch.is_grad_enabled():
+            u = torch.utils.checkpoint.checkpoint(_segment, u, seg, alpha, use_reentrant=False)
+        else:
+            u = _segment(u, seg, alpha)
+    return u

@@ -115,6 +115,22 @@ def tridDmtsvStridedBatchMixed(ctx, a, b, c, d, ndim, solvedim, dims, pads, max_
     return st, it.value, corr.value
 
 
+def tridDmtsvStridedBatchAdjoint(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndim, solvedim, dims,
+                                 pads):
+    """Adjoint of the strided solve (include/tridsolver_b200.h); abar, bbar,
+    cbar may be None. Returns the status code."""
+    return _lib.load().tridDmtsvStridedBatchAdjoint(
+        _ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(x), _addr(w), _addr(dbar), _addr(abar),
+        _addr(bbar), _addr(cbar), int(ndim), int(solvedim), _ints(dims), _ints(pads))
+
+
+def tridSmtsvStridedBatchAdjoint(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndim, solvedim, dims,
+                                 pads):
+    return _lib.load().tridSmtsvStridedBatchAdjoint(
+        _ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(x), _addr(w), _addr(dbar), _addr(abar),
+        _addr(bbar), _addr(cbar), int(ndim), int(solvedim), _ints(dims), _ints(pads))
+
+
 # ---- execution control -------------------------------------------------------
 
 def set_stream(stream):
