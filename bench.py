@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--cpu-steps", type=int, default=0, help="0 = as many as fit in ~10 s")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (sweep, ADI, precision, ragged, adjoint)")
     return ap.parse_args()
 
 
@@ -330,6 +332,260 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ---- the other configurations (reported beside the headline, not in `value`) ----
+
+def _timed(fn, reps, stream):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _system(shape, dt, dev, seed, margin_lo=None):
+    import torch
+    g = torch.Generator(device=dev).manual_seed(seed)
+    a = torch.rand(shape, generator=g, device=dev, dtype=dt) - 0.5
+    c = torch.rand(shape, generator=g, device=dev, dtype=dt) - 0.5
+    if margin_lo is None:
+        b = 1 + a.abs() + c.abs() + torch.rand(shape, generator=g, device=dev, dtype=dt)
+    else:
+        u = torch.rand(shape, generator=g, device=dev, dtype=torch.float64)
+        b = (a.abs() + c.abs() + 10.0 ** (margin_lo * (1 - u))).to(dt)
+    d = torch.randn(shape, generator=g, device=dev, dtype=dt)
+    return a, b, c, d
+
+
+def config_sweep(dev, hbm):
+    """Drop-in sweep: FP32/FP64, 256^3/512^3, x/y/z, overwrite and Inc."""
+    import torch
+    import tridsolver_b200 as tb
+    out = []
+    stream = torch.cuda.current_stream()
+    for n in (256, 512):
+        for dt, es, name in ((torch.float64, 8, "f64"), (torch.float32, 4, "f32")):
+            a, b, c, d = _system((n, n, n), dt, dev, n)
+            u = torch.randn_like(d)
+            dims = [n] * 3
+            for axis in range(3):
+                for inc in (False, True):
+                    if inc:
+                        fn = tb.tridDmtsvStridedBatchInc if es == 8 else tb.tridSmtsvStridedBatchInc
+                        call = lambda: fn(None, a, b, c, d, u, 3, axis, dims, dims)  # noqa: E731
+                    else:
+                        fn = tb.tridDmtsvStridedBatch if es == 8 else tb.tridSmtsvStridedBatch
+                        call = lambda: fn(None, a, b, c, d, 3, axis, dims, dims)  # noqa: E731
+                    ms = _timed(call, 10, stream)
+                    words = 6 if inc else 5
+                    gbs = words * es * n ** 3 / ms / 1e6
+                    out.append({"grid": n, "dtype": name, "axis": "xyz"[axis], "inc": inc,
+                                "ms": round(ms, 4), "elements_per_s": n ** 3 / ms * 1e3,
+                                "hbm_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
+                                "plan": tb.describe_plan(es, dims, axis)})
+            del a, b, c, d, u
+            torch.cuda.empty_cache()
+    return out
+
+
+def config_adi(dev, hbm, n=(256, 256, 256), steps=100, dtype="f64", alpha=1.0):
+    """ADI heat steps replayed from a CUDA graph of one timestep."""
+    import numpy as np
+    import torch
+    from tridsolver_b200.adi import ADIHeat
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    es = 8 if dtype == "f64" else 4
+    nz, ny, nx = n
+    g = torch.Generator(device=dev).manual_seed(3)
+    u = torch.randn((nz, ny, nx), generator=g, device=dev, dtype=dt)
+    u[0], u[-1], u[:, 0], u[:, -1], u[:, :, 0], u[:, :, -1] = 0, 0, 0, 0, 0, 0
+    lams = np.random.default_rng(4).uniform(0.1, 1.0, steps + 2)
+    sim = ADIHeat(u, lams, alpha=alpha)
+    sim.capture()
+    sim.reset_counter(0)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sim.run(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    elems = nx * ny * nz
+    words = 5 + 5 + 5 + 6  # RHS+coefficients, x, y, z-Inc (one shared coefficient set)
+    gbs = words * es * elems / ms / 1e6
+    return {"grid": [nx, ny, nz], "dtype": dtype, "steps": steps, "ms_per_step": round(ms, 4),
+            "elements_per_s": elems / ms * 1e3, "hbm_gbs": round(gbs, 1),
+            "frac": round(gbs / hbm, 4), "words_per_element_step": words,
+            "graph": "one timestep captured, replayed per step; lambda[step] read on the device",
+            "finite": bool(torch.isfinite(sim.u).all().item())}
+
+
+def config_precision(dev, n=512):
+    """FP32 storage + FP32 solve with on-chip FP64 refinement vs the plain FP64
+    solve, along x and z, margins log-uniform [10^lo, 1]."""
+    import torch
+    import tridsolver_b200 as tb
+    stream = torch.cuda.current_stream()
+    dims = [n] * 3
+    out = []
+    for lo in (-3, -2, -1, 0):
+        a, b, c, d = _system((n, n, n), torch.float64, dev, 7 - lo, margin_lo=lo if lo < 0 else None)
+        a32, b32, c32 = a.float(), b.float(), c.float()
+        del a, b, c
+        a64, b64, c64 = a32.double(), b32.double(), c32.double()
+        for axis in (0, 2):
+            x64 = d.clone()
+            tb.set_blocking(True)
+            tb.tridDmtsvStridedBatch(None, a64, b64, c64, x64, 3, axis, dims, dims)
+            xm = d.clone()
+            st, iters, corr = tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, xm, 3, axis, dims,
+                                                            dims, 12, 1e-12)
+            err = ((xm - x64).abs().max() / x64.abs().max()).item()
+            tb.set_blocking(False)
+            w = d.clone()
+            t64 = _timed(lambda: tb.tridDmtsvStridedBatch(None, a64, b64, c64, w, 3, axis, dims, dims),
+                         5, stream)
+            tmx = _timed(lambda: tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, w, 3, axis, dims,
+                                                               dims, 12, 1e-12), 5, stream)
+            out.append({"margin_min": 10.0 ** lo, "axis": "xyz"[axis], "status": st,
+                        "iterations": iters, "final_rel_correction": corr,
+                        "max_rel_error_vs_fp64": err, "fp64_ms": round(t64, 4),
+                        "mixed_ms": round(tmx, 4), "mixed_over_fp64_time": round(tmx / t64, 3)})
+            del x64, xm, w
+        del a32, b32, c32, a64, b64, c64, d
+        torch.cuda.empty_cache()
+    return out
+
+
+def config_ragged(dev, hbm, nsys=200000):
+    """200,000 systems, lengths floor(exp(U(ln 8, ln 16384))), one persistent launch."""
+    import numpy as np
+    import torch
+    import tridsolver_b200 as tb
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(0)
+    lengths = np.floor(np.exp(rng.uniform(np.log(8), np.log(16384), nsys))).astype(np.int64)
+    offs = torch.from_numpy(np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)).to(dev)
+    n = int(lengths.sum())
+    out = {"systems": nsys, "elements": n, "lengths": "floor(exp(U(ln 8, ln 16384))), seed 0"}
+    for dt, es, name in ((torch.float64, 8, "f64"), (torch.float32, 4, "f32")):
+        a, b, c, d = _system((n,), dt, dev, 11)
+        fn = tb.tridDmtsvRaggedBatch if es == 8 else tb.tridSmtsvRaggedBatch
+        ms = _timed(lambda: fn(None, a, b, c, d, offs, nsys), 5, stream)
+        gbs = (5 * es * n + 8 * (nsys + 1)) / ms / 1e6
+        out[name] = {"ms": round(ms, 4), "elements_per_s": n / ms * 1e3, "hbm_gbs": round(gbs, 1),
+                     "frac": round(gbs / hbm, 4), "rows_per_lane_by_class": tb.ragged_table(es)}
+        del a, b, c, d
+        torch.cuda.empty_cache()
+    return out
+
+
+def config_adjoint(dev, n=256, probes=1000):
+    """Adjoint along y on 256^3 FP64: time against the forward solve; gradient
+    entries against central finite differences (h = 1e-6) of L = sum(w x)."""
+    import torch
+    import tridsolver_b200 as tb
+    stream = torch.cuda.current_stream()
+    dims = [n] * 3
+    a, b, c, d = _system((n, n, n), torch.float64, dev, 21)
+    w = torch.randn_like(d)
+    x = d.clone()
+    tb.set_blocking(True)
+    tb.tridDmtsvStridedBatch(None, a, b, c, x, 3, 1, dims, dims)
+    grads = [torch.empty_like(d) for _ in range(4)]
+    tb.tridDmtsvStridedBatchAdjoint(None, a, b, c, x, w, grads[3], grads[0], grads[1], grads[2], 3, 1,
+                                    dims, dims)
+    tb.set_blocking(False)
+    xx = d.clone()
+    tf = _timed(lambda: tb.tridDmtsvStridedBatch(None, a, b, c, xx, 3, 1, dims, dims), 10, stream)
+    ta = _timed(lambda: tb.tridDmtsvStridedBatchAdjoint(None, a, b, c, x, w, grads[3], grads[0],
+                                                        grads[1], grads[2], 3, 1, dims, dims),
+                10, stream)
+    td_only = _timed(lambda: tb.tridDmtsvStridedBatchAdjoint(None, a, b, c, x, w, grads[3], None, None,
+                                                             None, 3, 1, dims, dims), 10, stream)
+    # finite differences: perturb one entry, solve twice; only the y-line of
+    # the perturbed entry changes, so the difference of L = sum(w x) is taken
+    # over that line (a global sum would bury it in summation roundoff)
+    tb.set_blocking(True)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    arrays = [a, b, c, d]
+    worst = 0.0
+    h = 1e-6
+    xp = torch.empty_like(d)
+    xm = torch.empty_like(d)
+    w3 = w.view(n, n, n)
+    for k in range(probes):
+        which = int(torch.randint(0, 4, (1,), generator=g))
+        idx = int(torch.randint(0, n ** 3, (1,), generator=g))
+        kz, rem = divmod(idx, n * n)
+        jy, ix = divmod(rem, n)
+        arr = arrays[which].view(-1)
+        old = arr[idx].item()
+        for sign, out in ((1.0, xp), (-1.0, xm)):
+            arr[idx] = old + sign * h
+            out.copy_(d)
+            tb.tridDmtsvStridedBatch(None, a, b, c, out, 3, 1, dims, dims)
+        arr[idx] = old
+        line = (xp.view(n, n, n)[kz, :, ix] - xm.view(n, n, n)[kz, :, ix])
+        fd = torch.dot(w3[kz, :, ix], line).item() / (2 * h)
+        gv = grads[which].view(-1)[idx].item()
+        worst = max(worst, abs(fd - gv) / max(1.0, abs(fd)))
+    return {"grid": dims, "axis": "y", "forward_ms": round(tf, 4), "adjoint_ms": round(ta, 4),
+            "adjoint_over_forward": round(ta / tf, 3), "adjoint_dbar_only_ms": round(td_only, 4),
+            "fd_probes": probes, "fd_worst_rel_error": worst,
+            "bytes_floor_ratio": "9 words (a,b,c,w,x in; 4 gradients out) vs 5 for the forward solve"}
+
+
+def config_adi_backprop(dev, n=64, steps=50, every=10):
+    """50-step ADI run backpropagated to the initial field and to each step's
+    lambda, checkpointing every 10 steps."""
+    import time
+    import torch
+    from tridsolver_b200.adi import adi_run
+    g = torch.Generator(device=dev).manual_seed(8)
+    u0 = torch.randn((n, n, n), generator=g, device=dev, dtype=torch.float64).requires_grad_(True)
+    lams = (0.1 + 0.9 * torch.rand(steps, generator=g, device=dev, dtype=torch.float64)).requires_grad_(True)
+    w = torch.randn((n, n, n), generator=g, device=dev, dtype=torch.float64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = (w * adi_run(u0, lams, checkpoint_every=every)).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    return {"grid": [n] * 3, "steps": steps, "checkpoint_every": every, "seconds": round(el, 3),
+            "grad_u0_finite": bool(torch.isfinite(u0.grad).all().item()),
+            "grad_lambda": [round(v, 6) for v in lams.grad[:5].tolist()]}
+
+
+def run_configs(dev, hbm):
+    import torch
+    import tridsolver_b200 as tb
+    tb.set_stream(torch.cuda.current_stream())
+    tb.set_blocking(False)
+    res = {}
+    for name, fn in (("sweep", lambda: config_sweep(dev, hbm)),
+                     ("adi_256_f64_100", lambda: config_adi(dev, hbm)),
+                     ("precision", lambda: config_precision(dev)),
+                     ("ragged", lambda: config_ragged(dev, hbm)),
+                     ("adi_512x512x128_f32_1000", lambda: config_adi(dev, hbm, (128, 512, 512), 1000,
+                                                                      "f32")),
+                     ("adjoint", lambda: config_adjoint(dev)),
+                     ("adi_backprop", lambda: config_adi_backprop(dev))):
+        try:
+            res[name] = fn()
+        except Exception as e:  # keep the headline line whatever happens here
+            res[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    tb.set_blocking(True)
+    return res
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -363,6 +619,10 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_configs:
+        import torch
+
+        line["configs"] = run_configs(torch.device("cuda", local_rank), peaks()[0])
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, info = cpu_reference_rate(args.n, args.cpu_planes, args.cpu_steps, args.dtype)
         line["cpu_baseline"] = dict(info, value=rate, unit=UNIT)

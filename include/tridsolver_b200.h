@@ -53,6 +53,30 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
 
+/* ---- ragged batches -------------------------------------------------------
+ * No counterpart in the reference. nsys independent contiguous systems of
+ * uneven lengths: system k is rows [offsets[k], offsets[k+1]) of a, b, c, d
+ * (device arrays; offsets: nsys+1 non-decreasing int64 on the device).
+ * x overwrites d. Bucketed by length on the device, then solved in one
+ * persistent launch: systems up to 512 (double) / 1024 (float) rows one per
+ * warp with a per-length-class rows-per-lane table (pure PCR up to 32 rows,
+ * the partition hybrid beyond), longer systems one per CTA (up to 16384
+ * rows; a longer system makes a blocking call return
+ * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
+EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *a, const double *b,
+                                           const double *c, double *d, const int64_t *offsets,
+                                           long long nsys);
+EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a, const float *b,
+                                           const float *c, float *d, const int64_t *offsets,
+                                           long long nsys);
+/* Times every rows-per-lane choice per length class on this device (uniform
+ * synthetic batches, about a second) and keeps the fastest for later ragged
+ * calls of that precision on the current device. */
+EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
+/* Copies the rows-per-lane table in use (one entry per length class
+ * ceil(log2 N) = 0, 1, ...) and returns the number of classes, or -1. */
+EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses);
+
 /* ---- ADI heat-diffusion timestep -----------------------------------------
  * No single counterpart in the reference: one timestep of its ADI
  * application (apps/adi/src/adi_cuda.cu:282-326, preproc.cu:40-90) on an

@@ -33,6 +33,10 @@ SYMBOLS = {
     "tridForcePlan": (_I, [_I, _I]),
     "tridForceSystemsPerBlock": (_I, [_I]),
     "tridDescribePlan": (_I, [_I, _I, _I, _IP, _IP, ctypes.c_char_p, _I]),
+    "tridDmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
+    "tridSmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
+    "tridRaggedAutotune": (_I, [_I]),
+    "tridRaggedTable": (_I, [_I, _IP, _I]),
     "tridDADIStep": (_I, [_P] * 7 + [ctypes.c_double, _I, _I, _I]),
     "tridSADIStep": (_I, [_P] * 7 + [ctypes.c_float, _I, _I, _I]),
     "tridDmtsvStridedBatchAdjoint": (_I, [_P] * 10 + [_I, _I, _IP, _IP]),

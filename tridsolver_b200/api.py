@@ -131,6 +131,33 @@ def tridSmtsvStridedBatchAdjoint(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndi
         _addr(bbar), _addr(cbar), int(ndim), int(solvedim), _ints(dims), _ints(pads))
 
 
+def tridDmtsvRaggedBatch(ctx, a, b, c, d, offsets, nsys):
+    """Ragged batch (include/tridsolver_b200.h): offsets is a device int64
+    array of nsys + 1 entries. Returns the status code."""
+    return _lib.load().tridDmtsvRaggedBatch(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                            _addr(offsets), int(nsys))
+
+
+def tridSmtsvRaggedBatch(ctx, a, b, c, d, offsets, nsys):
+    return _lib.load().tridSmtsvRaggedBatch(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                            _addr(offsets), int(nsys))
+
+
+def ragged_autotune(dtype_bytes):
+    st = _lib.load().tridRaggedAutotune(int(dtype_bytes))
+    if st != 0:
+        raise TridError(st, "tridRaggedAutotune")
+
+
+def ragged_table(dtype_bytes):
+    """Rows per lane by length class (index = ceil(log2 N)) for warp items."""
+    buf = (ctypes.c_int * 32)()
+    n = _lib.load().tridRaggedTable(int(dtype_bytes), buf, 32)
+    if n < 0:
+        raise TridError(TridStatus.INVALID_VALUE, "tridRaggedTable")
+    return list(buf[:n])
+
+
 # ---- execution control -------------------------------------------------------
 
 def set_stream(stream):
