@@ -53,6 +53,11 @@ EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
 
+/* Strided batches: 1 = load whole tiles with TMA (persistent, double
+ * buffered) wherever the alignment and size rules allow; 0 or -1 (default) =
+ * per-thread loads, which measure faster for rows of 32-64 bytes. */
+EXTERN_C tridStatus_t tridForceTma(int mode);
+
 /* ---- ragged batches -------------------------------------------------------
  * No counterpart in the reference. nsys independent contiguous systems of
  * uneven lengths: system k is rows [offsets[k], offsets[k+1]) of a, b, c, d

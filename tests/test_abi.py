@@ -75,6 +75,7 @@ def test_empty_problem_is_success_without_device():
     (8, [512, 512, 512], 0, "hybrid M=16 T=32 W=1 smem"),
     (8, [512, 512, 512], 2, "hybrid M=8 T=64 W=8"),
     (8, [512, 512, 512], 1, "hybrid M=8 T=64 W=8"),
+    (8, [256, 256, 256], 2, "hybrid M=8 T=32 W=16"),
     (8, [7, 512, 3], 1, "hybrid M=8 T=64 W=8"),
     (4, [512, 512, 512], 2, "hybrid M=16 T=32 W=16"),
     (8, [256, 256, 256], 1, "hybrid M=8 T=32 W=8"),

@@ -185,6 +185,22 @@ def test_every_family(dims, solvedim, family, m, dt, oracle, reference):
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("tma", [1, 0])
+@pytest.mark.parametrize("dims,solvedim", [([48, 37, 20], 1), ([48, 37, 20], 2), ([24, 300, 3], 1),
+                                           ([20, 3, 260], 2), ([12, 7, 513], 2), ([64, 40], 1),
+                                           ([8, 9, 16], 2)])
+def test_tma_tiles(dims, solvedim, tma, inc, dt, oracle, reference):
+    """TMA tile path against the per-thread-load path and the oracle: partial
+    groups of systems, lengths that end inside a box, two and three boxes."""
+    tb.force_tma(tma)
+    try:
+        _check(dims, solvedim, dt, inc, oracle, reference, seed=tma + 2 * inc)
+    finally:
+        tb.force_tma(-1)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
 @pytest.mark.parametrize("dims,solvedim", [([100000], 0), ([3, 20000], 1), ([2, 2, 9000], 2),
                                            ([70000, 3], 0)])
 def test_long_systems(dims, solvedim, dt, oracle, reference):

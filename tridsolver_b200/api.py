@@ -194,6 +194,13 @@ def force_systems_per_block(systems=0):
         raise TridError(st, "tridForceSystemsPerBlock")
 
 
+def force_tma(mode=-1):
+    """1: TMA tiles for strided batches wherever allowed; 0 / -1 (default): not."""
+    st = _lib.load().tridForceTma(int(mode))
+    if st != 0:
+        raise TridError(st, "tridForceTma")
+
+
 def describe_plan(dtype_bytes, dims, solvedim, pads=None):
     pads = dims if pads is None else pads
     buf = ctypes.create_string_buffer(128)

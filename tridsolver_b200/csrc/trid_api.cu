@@ -242,6 +242,12 @@ EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems) {
   return TRID_STATUS_SUCCESS;
 }
 
+EXTERN_C tridStatus_t tridForceTma(int mode) {
+  if (mode < -1 || mode > 1) return TRID_STATUS_INVALID_VALUE;
+  settings().force_tma = mode;
+  return TRID_STATUS_SUCCESS;
+}
+
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
                               const int *pads, char *buf, int buflen) {
   std::string desc;

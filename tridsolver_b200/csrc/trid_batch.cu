@@ -13,7 +13,7 @@ std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
   snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
-           smem ? " smem" : vec ? " vec" : "");
+           smem ? " smem" : vec ? " vec" : tma ? " tma" : "");
   return buf;
 }
 
@@ -88,7 +88,9 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
       } else {
         // at least 64 contiguous bytes per row: rows of a z solve are a whole
         // plane apart, and z throughput grows with the bytes per row access
-        const int wseg = 64 / (int)sizeof(R);
+        // rows a whole plane apart (>= 64 KiB: z solves) want 128 bytes per
+        // row and per warp load, others 64 (measured, see the plan table)
+        const int wseg = (p.stride * (long long)sizeof(R) >= (1LL << 16) ? 128 : 64) / (int)sizeof(R);
         int W = 256 / T > wseg ? 256 / T : wseg;
         const int wmin = 32 / T > 1 ? 32 / T : 1;
         const int n0p = pow2_ceil(p.n0);
@@ -98,6 +100,31 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         const int tmax = (T > 32 || M * (int)sizeof(R) <= 64) ? 512 : 256;
         if (W * T > tmax) W = tmax / T;
         plan.W = W;
+        // TMA tiles (two stages when they fit), at most 256 threads per CTA.
+        // Opt-in: with rows of 32-64 bytes the tile loads are limited by the
+        // rate of box rows, and measure slower than per-thread loads.
+        const int ft = honour_force ? st.force_tma : -1;
+        if (ft == 1 && (M == 8 || (M == 16 && sizeof(R) == 4)) && T <= 128) {
+          const int wmin_tma = 16 / (int)sizeof(R);
+          int wt = (honour_force && st.force_w > 0) ? st.force_w : 2 * wmin_tma;
+          if (!(honour_force && st.force_w > 0)) {
+            // widest group (up to 16) that keeps two stages and covers n0
+            for (int cand = wt * 2; cand <= 16; cand *= 2) {
+              int rb, nb, stg;
+              size_t sm;
+              if (cand * T > 256 || cand > n0p) break;
+              if (!tma_geometry<R>(p, p.u != nullptr, cand, rb, nb, stg, sm, T) || stg < 2) break;
+              wt = cand;
+            }
+          }
+          if (wt * T < 32) wt = 32 / T;
+          int rb, nb, stg;
+          size_t sm;
+          if (wt * T <= 256 && tma_geometry<R>(p, p.u != nullptr, wt, rb, nb, stg, sm, T)) {
+            plan.W = wt;
+            plan.tma = true;
+          }
+        }
       }
       return plan;
     }
@@ -151,6 +178,18 @@ static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cuda
     } else {
       contig_kernel<R, M, INC, false><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
     }
+  } else if (plan.tma) {
+    cudaError_t e = cudaErrorInvalidValue;
+    if constexpr (M == 8 || (M == 16 && sizeof(R) == 4)) {
+      if (plan.T <= 32)
+        e = launch_strided_tma<R, M, 2, INC>(p, plan, st);
+      else if (plan.T == 64)
+        e = launch_strided_tma<R, M, 4, INC>(p, plan, st);
+      else if constexpr (M == 8) {
+        if (plan.T == 128) e = launch_strided_tma<R, M, 8, INC>(p, plan, st);
+      }
+    }
+    if (e != cudaSuccess) return e;
   } else {
     cudaError_t e = cudaErrorInvalidValue;
     if (plan.T <= 32) {

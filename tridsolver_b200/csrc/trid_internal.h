@@ -18,6 +18,7 @@ struct Plan {
   int W = 1;                        // systems per block (strided hybrid)
   bool vec = false;                 // 16-byte vector loads (contiguous hybrid)
   bool smem = false;                // warp-per-system staging through shared memory
+  bool tma = false;                 // strided: TMA tiles, persistent, double-buffered
   std::string describe() const;
 };
 
@@ -28,6 +29,7 @@ struct Settings {
   int force_family = TRID_FAMILY_AUTO;
   int force_m = 0;
   int force_w = 0;
+  int force_tma = -1;  // -1 automatic, 0 off, 1 on where it applies
 };
 Settings &settings();
 
@@ -49,6 +51,14 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force = true
 // Enqueues the solve of batch p on `st` (no synchronisation).
 template <typename R, bool INC>
 cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
+
+// TMA tile geometry of a strided batch (trid_strided_tma.cu); false when TMA
+// does not apply (alignment, strides, length, shared-memory size).
+template <typename R>
+bool tma_geometry(const BatchArgs<R> &p, bool inc, int W, int &rows_box, int &nbox, int &stages,
+                  size_t &smem, int T);
+template <typename R, int M, int KR, bool INC>
+cudaError_t launch_strided_tma(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
 
 // Whether every pointer and every system start allows 16-byte vector access
 // (contiguous systems only).

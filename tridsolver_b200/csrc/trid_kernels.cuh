@@ -87,6 +87,44 @@ __device__ __forceinline__ void load_chunk(const BatchArgs<R> &p, long long base
     if (row0 + i == N - 1) rc[i] = R(0);
 }
 
+// Loads u at rows [row0, row0+M) for the Inc variants, with the inputs, so
+// its latency overlaps the solve (zero past the system end).
+template <typename R, int M, bool VEC>
+__device__ __forceinline__ void load_u(const BatchArgs<R> &p, long long base, int row0, bool active,
+                                       R (&uu)[M]) {
+  const int N = p.N;
+  if (VEC && active && row0 + M <= N) {
+    load_vec<R, M>(p.u + base + row0, uu);
+  } else {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int row = row0 + i;
+      uu[i] = (active && row < N) ? p.u[base + (long long)row * p.stride] : R(0);
+    }
+  }
+}
+
+// Writes u + x for rows [row0, row0+M) inside the system (Inc variants,
+// u loaded beforehand by load_u).
+template <typename R, int M, bool VEC>
+__device__ __forceinline__ void store_inc(const BatchArgs<R> &p, long long base, int row0,
+                                          bool active, const R (&uu)[M], const R (&x)[M]) {
+  if (!active) return;
+  const int N = p.N;
+  R v[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) v[i] = uu[i] + x[i];
+  if (VEC && row0 + M <= N) {
+    store_vec<R, M>(p.u + base + row0, v);
+  } else {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int row = row0 + i;
+      if (row < N) p.u[base + (long long)row * p.stride] = v[i];
+    }
+  }
+}
+
 // Writes x (in rd) for rows [row0, row0+M) that lie inside the system.
 template <typename R, int M, bool INC, bool VEC>
 __device__ __forceinline__ void store_chunk(const BatchArgs<R> &p, long long base, int row0,
@@ -132,6 +170,8 @@ __global__ void __launch_bounds__(128) contig_kernel(const BatchArgs<R> p, int T
   const int row0 = t * M;
   R ra[M], rb[M], rc[M], rd[M];
   load_chunk<R, M, VEC>(p, base, row0, active, ra, rb, rc, rd);
+  R uu[INC ? M : 1];
+  if constexpr (INC) load_u<R, M, VEC>(p, base, row0, active, uu);
   bool bad = false;
   chunk_forward<R, M>(ra, rb, rc, rd, bad);
   chunk_backward<R, M>(ra, rc, rd, bad);
@@ -140,7 +180,10 @@ __global__ void __launch_bounds__(128) contig_kernel(const BatchArgs<R> p, int T
   R y, z;
   reduced_solve<R>(top, bot, t, T, y, z, bad);
   chunk_substitute<R, M>(ra, rc, rd, y, z);
-  store_chunk<R, M, INC, VEC>(p, base, row0, active, rd);
+  if constexpr (INC)
+    store_inc<R, M, VEC>(p, base, row0, active, uu, rd);
+  else
+    store_chunk<R, M, false, VEC>(p, base, row0, active, rd);
   report_bad_pivot(bad && active, p.flag);
 }
 
@@ -377,6 +420,8 @@ __global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
   const int row0 = t * M;
   R ra[M], rb[M], rc[M], rd[M];
   load_chunk<R, M, false>(p, base, row0, active, ra, rb, rc, rd);
+  R uu[INC ? M : 1];
+  if constexpr (INC) load_u<R, M, false>(p, base, row0, active, uu);
   bool bad = false;
   chunk_forward<R, M>(ra, rb, rc, rd, bad);
   chunk_backward<R, M>(ra, rc, rd, bad);
@@ -384,7 +429,10 @@ __global__ void __launch_bounds__((KR >= 4 || M * sizeof(R) <= 64) ? 512 : 256)
   block_reduced_solve<R, KR>(sm, Row<R>{ra[0], rc[0], rd[0]}, Row<R>{ra[M - 1], rc[M - 1], rd[M - 1]},
                              s, t, T, W, y, z, bad);
   chunk_substitute<R, M>(ra, rc, rd, y, z);
-  store_chunk<R, M, INC, false>(p, base, row0, active, rd);
+  if constexpr (INC)
+    store_inc<R, M, false>(p, base, row0, active, uu, rd);
+  else
+    store_chunk<R, M, false, false>(p, base, row0, active, rd);
   report_bad_pivot(bad && active, p.flag);
 }
 
