@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--grid", default=None,
+                    help="X,Y,Z grid instead of n^3 (smaller cases for profiling; x fastest)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-planes", type=int, default=32,
                     help="slab thickness of the CPU sample (planes of n*n)")
@@ -199,8 +201,10 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     n = args.n
-    shape = (n, n, n)
-    dims = [n, n, n]
+    dims = [int(v) for v in args.grid.split(",")] if args.grid else [n, n, n]
+    if len(dims) != 3:
+        raise SystemExit("--grid takes X,Y,Z")
+    shape = tuple(reversed(dims))
     tdt = torch.float64 if args.dtype == "f64" else torch.float32
     es = 8 if args.dtype == "f64" else 4
     g = torch.Generator(device=dev).manual_seed(1234 + rank)
@@ -209,7 +213,7 @@ def run_ours(args, rank, world, local_rank):
     b = 1 + a.abs() + c.abs() + torch.rand(shape, generator=g, device=dev, dtype=tdt)
     d = torch.randn(shape, generator=g, device=dev, dtype=tdt)
     solve = tb.tridDmtsvStridedBatch if args.dtype == "f64" else tb.tridSmtsvStridedBatch
-    elems = n ** 3
+    elems = dims[0] * dims[1] * dims[2]
 
     stream = torch.cuda.current_stream()
     tb.set_stream(stream)
@@ -311,7 +315,7 @@ def run_ours(args, rank, world, local_rank):
         }
     dom = max(range(3), key=lambda i: axis_ms[i])
     dom_gbs = alg_bytes / (axis_ms[dom] / 1e3) / 1e9
-    key = f"{args.dtype}_n{n}_{names[dom]}"
+    key = f"{args.dtype}_n{n}_{names[dom]}" if not args.grid else None
     roofline = {"bound": "hbm", "achieved": round(dom_gbs, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(dom_gbs / hbm, 4),
                 "traffic": traffic.get(key),
@@ -321,9 +325,11 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
-            "config": {"workload": f"{n}^3 {args.dtype.upper()} tridDmtsvStridedBatch along x, y, z "
-                                   f"(one step = 3 solves of {n * n} systems of length {n}, d "
-                                   "overwritten, ADI order)",
+            "config": {"workload": (f"{n}^3 {args.dtype.upper()} tridDmtsvStridedBatch along x, y, z "
+                                    f"(one step = 3 solves of {n * n} systems of length {n}, d "
+                                    "overwritten, ADI order)") if not args.grid else
+                       (f"{'x'.join(map(str, dims))} {args.dtype.upper()} solves along x, y, z "
+                        "(profiling case, not the benchmark)"),
                        "grid": dims, "parallelism": f"replicas x{world} (systems sharded by rank)",
                        "l2": "inputs larger than L2 (each array "
                              f"{elems * es / 2**30:.2f} GiB); no flush"},

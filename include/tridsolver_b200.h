@@ -58,6 +58,12 @@ EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
  * per-thread loads, which measure faster for rows of 32-64 bytes. */
 EXTERN_C tridStatus_t tridForceTma(int mode);
 
+/* Strided batches of 64 < N <= 512 rows: -1 (default) = the persistent
+ * streaming kernel (groups of 128 bytes of neighbouring systems, loads kept
+ * in flight across groups) unless TMA is forced; 1 = always that kernel where
+ * it applies; 0 = the register-tile strided kernel. */
+EXTERN_C tridStatus_t tridForceStream(int mode);
+
 /* ---- ragged batches -------------------------------------------------------
  * No counterpart in the reference. nsys independent contiguous systems of
  * uneven lengths: system k is rows [offsets[k], offsets[k+1]) of a, b, c, d

@@ -73,12 +73,20 @@ def test_empty_problem_is_success_without_device():
 
 @pytest.mark.parametrize("dtype_bytes,dims,solvedim,expect", [
     (8, [512, 512, 512], 0, "hybrid M=16 T=32 W=1 smem"),
-    (8, [512, 512, 512], 2, "hybrid M=8 T=64 W=8"),
-    (8, [512, 512, 512], 1, "hybrid M=8 T=64 W=8"),
-    (8, [256, 256, 256], 2, "hybrid M=8 T=32 W=16"),
+    (8, [512, 512, 512], 2, "hybrid M=16 T=32 W=16 stream"),
+    (8, [512, 512, 512], 1, "hybrid M=16 T=32 W=16 stream"),
+    (8, [256, 256, 256], 2, "hybrid M=8 T=32 W=16 stream"),
     (8, [7, 512, 3], 1, "hybrid M=8 T=64 W=8"),
-    (4, [512, 512, 512], 2, "hybrid M=16 T=32 W=16"),
-    (8, [256, 256, 256], 1, "hybrid M=8 T=32 W=8"),
+    (8, [8, 512, 3], 1, "hybrid M=16 T=32 W=16 stream"),
+    (4, [512, 512, 512], 2, "hybrid M=16 T=32 W=32 stream"),
+    (4, [512, 512, 512], 1, "hybrid M=16 T=32 W=32 stream"),
+    (4, [256, 256, 256], 1, "hybrid M=8 T=32 W=32 stream"),
+    (4, [3, 100, 2], 1, "hybrid M=8 T=16 W=4"),
+    (4, [16, 100, 2], 1, "hybrid M=4 T=32 W=32 stream"),
+    (8, [256, 256, 256], 1, "hybrid M=8 T=32 W=16 stream"),
+    (8, [64, 65], 1, "hybrid M=4 T=32 W=16 stream"),
+    (8, [64, 64], 1, "hybrid M=8 T=8 W=32"),
+    (8, [8, 8, 1024], 2, "hybrid M=8 T=128 W=4"),
     (4, [1024, 8], 0, "hybrid M=32 T=32"),
     (8, [100000], 0, "long"),
     (8, [5, 7], 1, "hybrid M=8 T=1"),

@@ -201,6 +201,23 @@ def test_tma_tiles(dims, solvedim, tma, inc, dt, oracle, reference):
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("stream", [1, 0])
+@pytest.mark.parametrize("dims,solvedim", [([48, 37, 100], 2), ([24, 300, 3], 1), ([20, 3, 260], 2),
+                                           ([7, 130, 5], 1), ([64, 65], 1), ([5, 9, 512], 2),
+                                           ([33, 17, 129], 2), ([40, 257], 1)])
+def test_streaming_kernel(dims, solvedim, stream, inc, dt, oracle, reference):
+    """Persistent streaming strided kernel against the register-tile kernel
+    and the oracle: partial groups, every chunk size (M = 4, 8, 16), lengths
+    that end inside a chunk, groups fewer than the grid and many per CTA."""
+    tb.force_stream(stream)
+    try:
+        _check(dims, solvedim, dt, inc, oracle, reference, seed=3 + stream + 2 * inc)
+    finally:
+        tb.force_stream(-1)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
 @pytest.mark.parametrize("dims,solvedim", [([100000], 0), ([3, 20000], 1), ([2, 2, 9000], 2),
                                            ([70000, 3], 0)])
 def test_long_systems(dims, solvedim, dt, oracle, reference):

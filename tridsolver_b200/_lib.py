@@ -33,6 +33,7 @@ SYMBOLS = {
     "tridForcePlan": (_I, [_I, _I]),
     "tridForceSystemsPerBlock": (_I, [_I]),
     "tridForceTma": (_I, [_I]),
+    "tridForceStream": (_I, [_I]),
     "tridDescribePlan": (_I, [_I, _I, _I, _IP, _IP, ctypes.c_char_p, _I]),
     "tridDmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
     "tridSmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),

@@ -201,6 +201,14 @@ def force_tma(mode=-1):
         raise TridError(st, "tridForceTma")
 
 
+def force_stream(mode=-1):
+    """Strided batches of 64 < N <= 512: -1 (default) streaming kernel unless
+    TMA is forced, 1 always where it applies, 0 the register-tile kernel."""
+    st = _lib.load().tridForceStream(int(mode))
+    if st != 0:
+        raise TridError(st, "tridForceStream")
+
+
 def describe_plan(dtype_bytes, dims, solvedim, pads=None):
     pads = dims if pads is None else pads
     buf = ctypes.create_string_buffer(128)

@@ -248,6 +248,12 @@ EXTERN_C tridStatus_t tridForceTma(int mode) {
   return TRID_STATUS_SUCCESS;
 }
 
+EXTERN_C tridStatus_t tridForceStream(int mode) {
+  if (mode < -1 || mode > 1) return TRID_STATUS_INVALID_VALUE;
+  settings().force_stream = mode;
+  return TRID_STATUS_SUCCESS;
+}
+
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
                               const int *pads, char *buf, int buflen) {
   std::string desc;

@@ -13,7 +13,7 @@ std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
   snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
-           smem ? " smem" : vec ? " vec" : tma ? " tma" : "");
+           smem ? " smem" : vec ? " vec" : tma ? " tma" : streaming ? " stream" : "");
   return buf;
 }
 
@@ -100,6 +100,27 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         const int tmax = (T > 32 || M * (int)sizeof(R) <= 64) ? 512 : 256;
         if (W * T > tmax) W = tmax / T;
         plan.W = W;
+        // persistent streaming kernel for 64 < N <= 512: 128-byte row
+        // segments, 512 threads (32 chunks of FP64 rows, 16 of FP32 rows)
+        // and loads kept in flight across groups
+        const int fs = honour_force ? st.force_stream : -1;
+        const bool want_tma = honour_force && st.force_tma == 1;
+        const int fm = honour_force ? st.force_m : 0;
+        const int Ts = 32;
+        const int m_lo = 4;  // instantiated: 4, 8, 16
+        const bool fm_ok = fm == 0 || ((fm == m_lo || fm == 2 * m_lo || fm == 4 * m_lo) && Ts * fm >= N);
+        // (groups are always 128 bytes wide: automatic only when at least half
+        // of a group holds systems)
+        const int Ws = stream_width<R>(p.n0);
+        if ((fs == 1 || (fs == -1 && !want_tma && fm_ok && 2 * p.n0 >= Ws)) && N > 64 && N <= 512) {
+          int Ms = N <= Ts * m_lo ? m_lo : N <= 2 * Ts * m_lo ? 2 * m_lo : 4 * m_lo;
+          if (fm > 0 && fm_ok) Ms = fm;
+          plan.M = Ms;
+          plan.T = Ts;
+          plan.W = Ws;
+          plan.streaming = true;
+          return plan;
+        }
         // TMA tiles (two stages when they fit), at most 256 threads per CTA.
         // Opt-in: with rows of 32-64 bytes the tile loads are limited by the
         // rate of box rows, and measure slower than per-thread loads.
@@ -178,6 +199,10 @@ static cudaError_t launch_hybrid_m(const BatchArgs<R> &p, const Plan &plan, cuda
     } else {
       contig_kernel<R, M, INC, false><<<(unsigned)blocks, threads, 0, st>>>(p, plan.T);
     }
+  } else if (plan.streaming) {
+    cudaError_t e = cudaErrorInvalidValue;
+    if constexpr (M == 4 || M == 8 || M == 16) e = launch_strided_stream<R, M, INC>(p, plan, st);
+    if (e != cudaSuccess) return e;
   } else if (plan.tma) {
     cudaError_t e = cudaErrorInvalidValue;
     if constexpr (M == 8 || (M == 16 && sizeof(R) == 4)) {

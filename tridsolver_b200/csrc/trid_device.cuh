@@ -234,6 +234,15 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src,
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem_src), "r"(bytes)
                : "memory");
 }
+// Asynchronous copy of one element (4 or 8 bytes, naturally aligned).
+template <typename R> __device__ __forceinline__ void cp_async_elem(R *smem_dst, const R *gmem_src) {
+  static_assert(sizeof(R) == 4 || sizeof(R) == 8, "4- or 8-byte elements");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  if constexpr (sizeof(R) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }

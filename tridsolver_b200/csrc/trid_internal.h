@@ -19,6 +19,7 @@ struct Plan {
   bool vec = false;                 // 16-byte vector loads (contiguous hybrid)
   bool smem = false;                // warp-per-system staging through shared memory
   bool tma = false;                 // strided: TMA tiles, persistent, double-buffered
+  bool streaming = false;           // strided: persistent streaming kernel (T = 32)
   std::string describe() const;
 };
 
@@ -30,6 +31,7 @@ struct Settings {
   int force_m = 0;
   int force_w = 0;
   int force_tma = -1;  // -1 automatic, 0 off, 1 on where it applies
+  int force_stream = -1;  // -1 automatic, 0 off, 1 on where it applies
 };
 Settings &settings();
 
@@ -59,6 +61,12 @@ bool tma_geometry(const BatchArgs<R> &p, bool inc, int W, int &rows_box, int &nb
                   size_t &smem, int T);
 template <typename R, int M, int KR, bool INC>
 cudaError_t launch_strided_tma(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
+
+// Streaming strided kernel (trid_strided_stream.cu): group width for n0
+// systems along the fastest dimension, and its launcher.
+template <typename R> int stream_width(long long n0);
+template <typename R, int M, bool INC>
+cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
 
 // Whether every pointer and every system start allows 16-byte vector access
 // (contiguous systems only).

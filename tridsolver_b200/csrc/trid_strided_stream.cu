@@ -1,0 +1,311 @@
+// Strided batches (solvedim >= 1), streaming form of the hybrid solve.
+//
+// Why a second strided kernel: strided_kernel holds a whole chunk (M rows of
+// a, b, c, d) in registers, so a 512-row FP64 group of 8 systems already
+// takes a 512-thread CTA with ~100 registers, i.e. one CTA per SM with no
+// other CTA to hide its load latency (measured: the same access pattern with
+// no arithmetic reaches 61% of the copy bandwidth at one CTA per SM, 104%
+// with many). Rows a whole plane apart (z solves) are in addition limited
+// per 64-byte row segment (about 50 G segments/s); 128-byte segments reach
+// 97% of the copy bandwidth.
+//
+// Here a persistent CTA walks over groups of W systems with W * sizeof(R) =
+// 128 bytes (16 FP64 / 32 FP32 systems) and T = 32 chunks of M rows each
+// (one warp per system for the reduced solve). Each thread
+//   1. streams its chunk's rows through a D-deep register window that runs
+//      on into the next group's first rows, so loads stay in flight across
+//      the reduced solve and the stores. When the rows of a system are less
+//      than 64 KiB apart (y solves), some lanes of each warp also ask L2 for
+//      the rows PF steps ahead (no registers). For rows a plane apart (z)
+//      that costs more in address translation than it saves, so it is off;
+//   2. runs the forward half of the chunk elimination row by row, keeping
+//      a', c' (and d' when SD, to make room for a deeper window) in its own
+//      shared-memory slots [j * BS + tid] (no other thread reads them, so the
+//      sweep needs no barrier; BS is a compile-time constant, so every slot
+//      has an immediate address);
+//   3. recovers the chunk's top reduced row with a backward recursion that
+//      only carries one running row;
+//   4. after the block-wide reduced solve, back-substitutes
+//          x_i = d'_i - a'_i x_first - c'_i x_{i+1}
+//      from the chunk's last row up, and stores.
+// Inc variants read u after the reduced solve, so its latency overlaps the
+// back-substitution. Every element is read once and written once.
+#include <cuda_runtime.h>
+
+#include "trid_internal.h"
+
+namespace trid {
+
+namespace {
+
+template <typename R> constexpr int stream_w() { return 128 / (int)sizeof(R); }
+template <typename R> constexpr int stream_bs() { return 32 * stream_w<R>(); }
+
+// Row `row` at element offset o: identity rows outside the system, a[0] and
+// c[N-1] forced to zero.
+template <typename R>
+__device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, long long o, bool valid,
+                                                int row, R &a, R &b, R &c, R &d) {
+  if (valid) {
+    a = row == 0 ? R(0) : __ldg(p.a + o);
+    b = __ldg(p.b + o);
+    c = row == p.N - 1 ? R(0) : __ldg(p.c + o);
+    d = __ldg(p.d_in + o);
+  } else {
+    a = R(0);
+    b = R(1);
+    c = R(0);
+    d = R(0);
+  }
+}
+
+}  // namespace
+
+template <typename R, int M, int D, bool SD, int PF, bool INC>
+__global__ void __launch_bounds__(stream_bs<R>(), 1)
+    strided_stream_kernel(const BatchArgs<R> p, long long ngx, long long ngroups) {
+  static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
+  static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
+  constexpr int W = stream_w<R>();
+  constexpr int T = 32;
+  constexpr int BS = W * T;
+  constexpr int RED = (6 * T * (W + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
+  extern __shared__ __align__(16) unsigned char stream_smem[];
+  R *red = reinterpret_cast<R *>(stream_smem);
+  const int tid = threadIdx.x;
+  R *saf = red + RED + tid;             // a' of row j at [j * BS]
+  R *scf = red + RED + M * BS + tid;    // c'
+  R *sdf = red + RED + 2 * M * BS + tid;  // d' (SD)
+  const int s = tid % W;
+  const int t = tid / W;
+  const int N = p.N;
+  const int row0 = t * M;
+  const long long stride = p.stride;
+
+  // element offset of this thread's first chunk row in group g (0 if none)
+  auto group_first = [&](long long g, bool &act) -> long long {
+    const long long gx = g % ngx;
+    const long long i1 = g / ngx;
+    const long long i0 = gx * W + s;
+    act = g < ngroups && i0 < p.n0;
+    return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
+  };
+
+  // L2 prefetch lanes (PF > 0): lane l < 16 covers one end (first or last
+  // system) of the row segment of one array for one of the warp's two chunks
+  const int lane = tid & 31;
+  const bool pf_lane = PF > 0 && lane < 16;
+  const int pq = (lane >> 1) & 3;
+  const int pt = (tid >> 5) * (32 / W) + (lane >> 3);
+  const R *pbase = pq == 0 ? p.a : pq == 1 ? p.b : pq == 2 ? p.c : p.d_in;
+  auto pf_first = [&](long long g, bool &ok) -> long long {
+    const long long gx = g % ngx;
+    const long long i1 = g / ngx;
+    const long long left = p.n0 - gx * W;
+    const long long i0 = gx * W + ((lane & 1) ? (left < W ? left : W) - 1 : 0);
+    ok = pf_lane && g < ngroups;
+    return ok ? i0 * p.st0 + i1 * p.st1 + (long long)pt * M * stride : 0;
+  };
+
+  R pa[D], pb[D], pc[D], pd[D];
+  long long g = blockIdx.x;
+  bool act;
+  long long first = group_first(g, act);
+  long long lo = first;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    stream_load_row<R>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
+    lo += stride;
+  }
+  bool pok = false;
+  long long po = 0;
+  if constexpr (PF > 0) po = pf_first(g, pok) + (long long)PF * stride;
+
+  bool bad = false;
+  for (; g < ngroups; g += gridDim.x) {
+    bool actn;
+    const long long firstn = group_first(g + gridDim.x, actn);
+    long long ln = firstn;
+    bool pokn = false;
+    long long pon = 0;
+    if constexpr (PF > 0) pon = pf_first(g + gridDim.x, pokn);
+
+    // forward half of the chunk elimination, streamed row by row
+    R rd[SD ? 1 : M];
+    R ap = R(0), cp = R(0), dp = R(0);
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int k = j % D;
+      const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
+      if (j + D < M) {
+        const int row = row0 + j + D;
+        stream_load_row<R>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        lo += stride;
+      } else {
+        const int row = row0 + j + D - M;
+        stream_load_row<R>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        ln += stride;
+      }
+      if constexpr (PF > 0) {
+        if (j + PF < M) {
+          if (pok && pt * M + j + PF < N) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(pbase + po));
+          po += stride;
+        } else {
+          if (pokn && pt * M + j + PF - M < N) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(pbase + pon));
+          pon += stride;
+        }
+      }
+      R af, cf, df;
+      if (j < 2) {
+        const R r = rcp(b);
+        bad |= !finite_rcp(r);
+        af = a * r;
+        cf = c * r;
+        df = d * r;
+      } else {
+        const R r = rcp(b - a * cp);
+        bad |= !finite_rcp(r);
+        df = r * (d - a * dp);
+        af = -r * a * ap;
+        cf = r * c;
+      }
+      saf[j * BS] = af;
+      scf[j * BS] = cf;
+      if constexpr (SD)
+        sdf[j * BS] = df;
+      else
+        rd[j] = df;
+      ap = af;
+      cp = cf;
+      dp = df;
+    }
+    auto dval = [&](int j) -> R {
+      if constexpr (SD)
+        return sdf[j * BS];
+      else
+        return rd[j];
+    };
+
+    // backward half: carry one running row from row M-2 up to row 1, then
+    // fold it into row 0 to get the chunk's top reduced row
+    R A = saf[(M - 2) * BS], C = scf[(M - 2) * BS], Dd = dval(M - 2);
+#pragma unroll
+    for (int j = M - 3; j >= 1; --j) {
+      const R cj = scf[j * BS];
+      Dd = dval(j) - cj * Dd;
+      A = saf[j * BS] - cj * A;
+      C = -cj * C;
+    }
+    const R a0 = saf[0], c0 = scf[0];
+    const R r0 = rcp(R(1) - c0 * A);
+    bad |= !finite_rcp(r0);
+    const Row<R> top{r0 * a0, -r0 * c0 * C, r0 * (dval(0) - c0 * Dd)};
+    const Row<R> bot{ap, cp, dp};
+    R y, z;
+    block_reduced_solve<R, 2>(red, top, bot, s, t, T, W, y, z, bad);
+
+    // Inc: u is read now, its latency overlapping the back-substitution
+    R uu[INC ? M : 1];
+    if constexpr (INC) {
+      long long o = first;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        uu[j] = (act && row0 + j < N) ? __ldg(p.u + o) : R(0);
+        o += stride;
+      }
+    }
+
+    // back-substitution with the forward rows, stored as it goes (last row
+    // first)
+    long long o = first + (long long)(M - 1) * stride;
+    R x = z;
+#pragma unroll
+    for (int j = M - 1; j >= 0; --j) {
+      if (j < M - 1) x = j == 0 ? y : dval(j) - saf[j * BS] * y - scf[j * BS] * x;
+      if (act && row0 + j < N) {
+        if constexpr (INC)
+          p.u[o] = uu[j] + x;
+        else
+          p.d_out[o] = x;
+      }
+      o -= stride;
+    }
+    first = firstn;
+    act = actn;
+    lo = ln;
+    if constexpr (PF > 0) {
+      po = pon;
+      pok = pokn;
+    }
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+// Group width of the streaming kernel (128 bytes of neighbouring systems).
+template <typename R> int stream_width(long long n0) {
+  (void)n0;
+  return stream_w<R>();
+}
+
+// Window depth, d' placement and L2 prefetch distance by element type and
+// chunk size, from measurements on 256^3 and 512^3 grids (fraction of the
+// copy bandwidth, y / z):
+//   FP64 M=16: D=4, prefetch 8 rows ahead: 0.99 / 0.77 (D=8 with d' in
+//              shared memory spills registers: 0.82 / 0.58);
+//   FP64 M=8:  D=8: 0.91 / 0.82 (D=4: 0.77 / 0.71);
+//   FP32 M=16: D=4, prefetch 12 rows ahead: 0.87 / 0.71 (D=8 spills).
+// The prefetch is used only for y-like layouts (see launch_strided_stream).
+template <typename R, int M> constexpr int stream_window() { return (sizeof(R) == 8 && M == 8) ? 8 : 4; }
+template <typename R, int M> constexpr bool stream_sd() { return false; }
+template <typename R, int M> constexpr int stream_prefetch() {
+  return stream_window<R, M>() >= M ? 0 : sizeof(R) == 8 ? 8 : (M >= 16 ? 12 : M);
+}
+
+template <typename R, int M, bool INC, int PF>
+static cudaError_t launch_stream_pf(const BatchArgs<R> &p, cudaStream_t st) {
+  constexpr int W = stream_w<R>();
+  constexpr int BS = stream_bs<R>();
+  constexpr int D = stream_window<R, M>();
+  constexpr bool SD = stream_sd<R, M>();
+  const size_t red = ((size_t)6 * 32 * (W + 1) * sizeof(R) + 15) / 16 * 16;
+  const size_t smem = red + (size_t)(SD ? 3 : 2) * M * BS * sizeof(R);
+  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long ngx = (p.n0 + W - 1) / W;
+  const long long ngroups = ngx * (p.nsys / p.n0);
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BS, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const long long cap = (long long)sms * per_sm;
+  const long long grid = ngroups < cap ? ngroups : cap;
+  kern<<<(unsigned)grid, BS, smem, st>>>(p, ngx, ngroups);
+  return cudaGetLastError();
+}
+
+template <typename R, int M, bool INC>
+cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
+  if (plan.T != 32 || plan.W != stream_w<R>() || p.N > 32 * M) return cudaErrorInvalidValue;
+  constexpr int PF = stream_prefetch<R, M>();
+  // L2 prefetch only where the rows of a system are less than 64 KiB apart
+  if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16)) return launch_stream_pf<R, M, INC, PF>(p, st);
+  return launch_stream_pf<R, M, INC, 0>(p, st);
+}
+
+#define INST_STREAM(R, M)                                                                       \
+  template cudaError_t launch_strided_stream<R, M, false>(const BatchArgs<R> &, const Plan &,    \
+                                                           cudaStream_t);                      \
+  template cudaError_t launch_strided_stream<R, M, true>(const BatchArgs<R> &, const Plan &,     \
+                                                          cudaStream_t);
+INST_STREAM(double, 4)
+INST_STREAM(double, 8)
+INST_STREAM(double, 16)
+INST_STREAM(float, 4)
+INST_STREAM(float, 8)
+INST_STREAM(float, 16)
+template int stream_width<double>(long long);
+template int stream_width<float>(long long);
+
+}  // namespace trid
