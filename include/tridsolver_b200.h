@@ -131,12 +131,16 @@ EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const TridParams *ctx, const 
  * No counterpart in the reference. Solves T x = d where a, b, c are stored in
  * FP32 (the system is exactly those values, promoted to FP64) and d is FP64;
  * x overwrites d. The solve runs in FP32; only the residual r = d - T x and
- * the accumulation x += dx run in FP64, repeated on chip until
- * max|dx| <= tol * max|x| for every system or max_iters FP32 solves. One pass
- * over memory: 28 bytes per element against 40 for tridDmtsvStridedBatch.
+ * the accumulation x += dx run in FP64. The FP32 factorisation is computed
+ * once and reused by every refinement pass, all on chip, until the estimated
+ * relative error of x is at most tol for every system, or max_iters FP32
+ * solves. The estimate is the a-posteriori bound of a contraction:
+ * rho / (1 - rho) * max|dx_k| / max|x|, with rho = max|dx_k| / max|dx_{k-1}|
+ * (max|dx_k| / max|x| itself while rho is unknown or >= 1/2). One pass over
+ * memory: 28 bytes per element against 40 for tridDmtsvStridedBatch.
  * Blocking calls report the largest iteration count and the largest final
- * relative correction over all systems in *iters_out / *correction_out (-1
- * when not blocking). Supports N <= 512 (longer systems return
+ * error estimate over all systems in *iters_out / *correction_out (-1 when
+ * not blocking). Supports N <= 512 (longer systems return
  * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
 EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const float *a,
                                                  const float *b, const float *c, double *d,

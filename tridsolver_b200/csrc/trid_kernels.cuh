@@ -202,6 +202,28 @@ template <typename R, int M> struct SmemLayout {
   static constexpr int BUF = 32 * ROW;           // one array of one system
 };
 
+// Stores M elements of a padded shared-memory chunk row as 16-byte units.
+template <typename R, int M>
+__device__ __forceinline__ void sts_row(R *row, const R (&v)[M]) {
+  using Vt = typename Vec16<R>::T;
+  constexpr int n = Vec16<R>::n;
+  Vt *q = reinterpret_cast<Vt *>(row);
+#pragma unroll
+  for (int i = 0; i < M / n; ++i) {
+    Vt x;
+    if constexpr (n == 2) {
+      x.x = v[2 * i];
+      x.y = v[2 * i + 1];
+    } else {
+      x.x = v[4 * i];
+      x.y = v[4 * i + 1];
+      x.z = v[4 * i + 2];
+      x.w = v[4 * i + 3];
+    }
+    q[i] = x;
+  }
+}
+
 template <typename R, int M>
 __device__ __forceinline__ void lds_row(const R *row, R (&v)[M]) {
   using Vt = typename Vec16<R>::T;

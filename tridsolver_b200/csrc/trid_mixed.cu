@@ -44,14 +44,99 @@ struct MixedStats {
 };
 static __device__ MixedStats g_mixed_stats;
 
+// Only values above the current maximum are sent as atomics, so the one
+// shared word is mostly read, not contended.
 __device__ __forceinline__ void mixed_report(int iters, double rel) {
-  atomicMax(&g_mixed_stats.iters, (unsigned)iters);
-  atomicMax(&g_mixed_stats.corr_bits, (unsigned long long)__double_as_longlong(rel));
+  if ((unsigned)iters > *reinterpret_cast<volatile unsigned *>(&g_mixed_stats.iters))
+    atomicMax(&g_mixed_stats.iters, (unsigned)iters);
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(rel);
+  if (bits > *reinterpret_cast<volatile unsigned long long *>(&g_mixed_stats.corr_bits))
+    atomicMax(&g_mixed_stats.corr_bits, bits);
+}
+
+// Estimated relative error of x after a correction of max-norm dmax, the
+// previous correction having been dprev (0 before the first refinement):
+// refinement contracts the error by about rho = dmax / dprev per pass, so
+// the error left is about rho / (1 - rho) * dmax (the a-posteriori bound of
+// a contraction). Without a usable rho the correction itself is the
+// estimate, as is any rho >= 1/2.
+__device__ __forceinline__ double mixed_error_estimate(float dmax, float dprev, double xmax) {
+  if (!(xmax > 0.0)) return 0.0;
+  double est = (double)dmax;
+  if (dprev > 0.f && dmax < 0.5f * dprev) {
+    const double rho = (double)dmax / (double)dprev;
+    est = est * rho / (1.0 - rho);
+  }
+  return est / xmax;
 }
 
 __device__ __forceinline__ long long mixed_base(const MixedArgs &p, long long s) {
   const long long i1 = s / p.n0;
   return (s - i1 * p.n0) * p.st0 + i1 * p.st1;
+}
+
+// Shared-memory chunk rows without padding: lane l's row is U = M*sizeof/16
+// units of 16 bytes, and unit u is stored at position u ^ swz(l), so the
+// 16-byte accesses of any 8 consecutive lanes to their own rows (the width of
+// one shared-memory wavefront) fall on 8 distinct bank groups.
+template <typename R, int M> struct Swz {
+  static constexpr int V = 16 / (int)sizeof(R);  // elements per unit
+  static constexpr int U = M / V;                 // units per row
+  static_assert(U >= 1 && (U & (U - 1)) == 0 && U <= 8, "row of 1..8 units");
+  __device__ static __forceinline__ int swz(int l) { return ((l * U) >> 3) & (U - 1); }
+  // element offset of element e of the system (lane e / M) in the tile
+  __device__ static __forceinline__ int off(int e) {
+    const int l = e / M, u = (e % M) / V;
+    return (l * U + (u ^ swz(l))) * V + e % V;
+  }
+  __device__ static __forceinline__ int unit(int l, int u) { return (l * U + (u ^ swz(l))) * V; }
+};
+
+template <typename R, int M>
+__device__ __forceinline__ void lds_swz(const R *tile, int l, R (&v)[M]) {
+  using S = Swz<R, M>;
+  using Vt = typename Vec16<R>::T;
+#pragma unroll
+  for (int u = 0; u < S::U; ++u) {
+    const Vt x = *reinterpret_cast<const Vt *>(tile + S::unit(l, u));
+    if constexpr (S::V == 2) {
+      v[2 * u] = x.x;
+      v[2 * u + 1] = x.y;
+    } else {
+      v[4 * u] = x.x;
+      v[4 * u + 1] = x.y;
+      v[4 * u + 2] = x.z;
+      v[4 * u + 3] = x.w;
+    }
+  }
+}
+
+template <typename R, int M>
+__device__ __forceinline__ void sts_swz(R *tile, int l, const R (&v)[M]) {
+  using S = Swz<R, M>;
+  using Vt = typename Vec16<R>::T;
+#pragma unroll
+  for (int u = 0; u < S::U; ++u) {
+    Vt x;
+    if constexpr (S::V == 2) {
+      x.x = v[2 * u];
+      x.y = v[2 * u + 1];
+    } else {
+      x.x = v[4 * u];
+      x.y = v[4 * u + 1];
+      x.z = v[4 * u + 2];
+      x.w = v[4 * u + 3];
+    }
+    *reinterpret_cast<Vt *>(tile + S::unit(l, u)) = x;
+  }
+}
+
+// Approximate FP32 reciprocal (rcp.approx, within one ulp): the FP32
+// factorisation only has to be good enough for refinement to converge.
+__device__ __forceinline__ float rcp_fast(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
 }
 
 // FP32 solve of T dx = r for one chunk of M rows given FP32 coefficients
@@ -72,30 +157,61 @@ __device__ __forceinline__ void fp32_chunk_solve(float (&wa)[M], float (&wb)[M],
 // Contiguous systems (stride 1), one warp per system, 16-byte aligned starts.
 // The warp stages a, b, c (FP32) and d (FP64) through shared memory with
 // coalesced 16-byte cp.async copies into padded rows (one spare 16-byte unit
-// per chunk row), as contig_smem_kernel does.
+// per chunk row, so a lane's 16-byte reads of its own row are conflict-free),
+// as contig_smem_kernel does.
+//
+// The FP32 solve is factored once: the first pass records, per row, the
+// pivot reciprocal r and the forward-eliminated a' (shared memory, next to
+// the fixed coefficients; c' = r c is recomputed), and per lane the reduced
+// system's PCR coefficients (registers). Every refinement pass then only applies them to
+// the FP32-rounded FP64 residual:
+//   forward   d'_i = r_i (d_i - a_i d'_{i-1})
+//   backward  the chunk's top reduced right-hand side (one running value)
+//   reduced   de <- (de - al_l de_left - ga_l de_right) r_l per PCR level
+//   back-substitution  dx_i = d'_i - a'_i dx_first - c'_i dx_{i+1}
+// which is a few FP32 operations per row instead of a fresh elimination.
 template <int M>
-__global__ void __launch_bounds__(128) mixed_contig_kernel(const MixedArgs p) {
-  constexpr int RF = M + 4;          // padded FP32 chunk row
-  constexpr int RD = M + 2;          // padded FP64 chunk row
-  constexpr int BF = 32 * RF;        // floats per FP32 tile
-  constexpr int BD = 32 * RD;        // doubles per FP64 tile
+__global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p) {
+  static_assert(M % 4 == 0 && M >= 8, "rows per lane");
+  using SF = Swz<float, M>;
+  using SD = Swz<double, M>;
+  constexpr int BF = 32 * M;    // floats per FP32 tile
+  constexpr int BD = 32 * M;    // doubles per FP64 tile
+  constexpr int NT = 5;         // FP32 tiles: a, b, c (fixed), r, a' (c' = r c is recomputed)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char *wbase = smem_raw + (threadIdx.x >> 5) * (3 * BF * 4 + BD * 8);
+  unsigned char *wbase = smem_raw + (threadIdx.x >> 5) * (NT * BF * 4 + BD * 8);
   float *ta = reinterpret_cast<float *>(wbase);
   float *tb = ta + BF;
   float *tc = tb + BF;
-  double *td = reinterpret_cast<double *>(wbase + 3 * BF * 4);
+  float *tr = tc + BF;
+  float *tfa = tr + BF;
+  double *td = reinterpret_cast<double *>(wbase + NT * BF * 4);
   const int lane = threadIdx.x & 31;
   const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (s >= p.nsys) return;  // uniform per warp
   const long long base = mixed_base(p, s);
   const int N = p.N;
-  {
+  const bool full = N == 32 * M;  // every lane's chunk full: unrolled copies
+  if (full) {
+#pragma unroll
+    for (int k = 0; k < M / 4; ++k) {
+      const int e = 4 * (lane + 32 * k);
+      const int o = SF::off(e);
+      cp_async16(ta + o, p.a + base + e, 16);
+      cp_async16(tb + o, p.b + base + e, 16);
+      cp_async16(tc + o, p.c + base + e, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < M / 2; ++k) {
+      const int e = 2 * (lane + 32 * k);
+      cp_async16(td + SD::off(e), p.d + base + e, 16);
+    }
+  } else {
     const int nu = (N + 3) / 4;  // FP32 units of 4
     for (int un = lane; un < nu; un += 32) {
       const int e = un * 4;
       const int left = (N - e) >= 4 ? 16 : (N - e) * 4;
-      const int o = e + (e / M) * 4;
+      const int o = SF::off(e);
       cp_async16(ta + o, p.a + base + e, left);
       cp_async16(tb + o, p.b + base + e, left);
       cp_async16(tc + o, p.c + base + e, left);
@@ -103,26 +219,24 @@ __global__ void __launch_bounds__(128) mixed_contig_kernel(const MixedArgs p) {
     const int nud = (N + 1) / 2;  // FP64 units of 2
     for (int un = lane; un < nud; un += 32) {
       const int e = un * 2;
-      cp_async16(td + e + (e / M) * 2, p.d + base + e, (N - e) >= 2 ? 16 : 8);
+      cp_async16(td + SD::off(e), p.d + base + e, (N - e) >= 2 ? 16 : 8);
     }
   }
   cp_async_wait_all();
   __syncwarp();
 
   const int row0 = lane * M;
-  double d64[M], x64[M];
-#pragma unroll
-  for (int i = 0; i < M; ++i) {
-    d64[i] = row0 + i < N ? td[lane * RD + i] : 0.0;
-    x64[i] = 0.0;
-  }
-  // FP32 coefficients of this lane's rows (16-byte reads of its padded row,
-  // conflict-free across neighbouring lanes), identity past the end, a[0]
-  // and c[N-1] zero
-  auto coef = [&](float (&wa)[M], float (&wb)[M], float (&wc)[M]) {
-    lds_row<float, M>(ta + lane * RF, wa);
-    lds_row<float, M>(tb + lane * RF, wb);
-    lds_row<float, M>(tc + lane * RF, wc);
+  bool bad = false;
+
+  // ---- first pass: fix the coefficients (identity rows past the end, a[0]
+  // and c[N-1] zero), factor, and solve T x = (float)d
+  float wa[M], wb[M], wc[M], wd[M];
+  lds_swz<float, M>(ta, lane, wa);
+  lds_swz<float, M>(tb, lane, wb);
+  lds_swz<float, M>(tc, lane, wc);
+  double dd[M];
+  lds_swz<double, M>(td, lane, dd);
+  if (row0 == 0 || row0 + M >= N) {  // chunks holding row 0, row N-1 or rows past the end
 #pragma unroll
     for (int i = 0; i < M; ++i) {
       const int row = row0 + i;
@@ -130,64 +244,216 @@ __global__ void __launch_bounds__(128) mixed_contig_kernel(const MixedArgs p) {
         wa[i] = 0.f;
         wb[i] = 1.f;
         wc[i] = 0.f;
+        dd[i] = 0.0;
       }
       if (row == 0) wa[i] = 0.f;
       if (row == N - 1) wc[i] = 0.f;
     }
-  };
-  bool bad = false;
-  int it = 0;
-  double rel = 0.0;
-  for (;;) {
-    float wa[M], wb[M], wc[M], wd[M];
-    coef(wa, wb, wc);
-    if (it == 0) {
+    sts_swz<float, M>(ta, lane, wa);
+    sts_swz<float, M>(tb, lane, wb);
+    sts_swz<float, M>(tc, lane, wc);
+    sts_swz<double, M>(td, lane, dd);
+  }
 #pragma unroll
-      for (int i = 0; i < M; ++i) wd[i] = (float)d64[i];
+  for (int i = 0; i < M; ++i) wd[i] = (float)dd[i];
+  float rr[M];
+  float psum = 0.f;  // sum of |pivot reciprocals|: not finite iff some pivot is 0 or NaN
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    if (i < 2) {
+      const float r = rcp_fast(wb[i]);
+      psum += fabsf(r);
+      rr[i] = r;
+      wa[i] *= r;
+      wc[i] *= r;
+      wd[i] *= r;
     } else {
-      double xl = __shfl_up_sync(FULL_MASK, x64[M - 1], 1);
-      double xr = __shfl_down_sync(FULL_MASK, x64[0], 1);
-      if (lane == 0) xl = 0.0;
-      if (lane == 31) xr = 0.0;
-#pragma unroll
-      for (int i = 0; i < M; ++i) {
-        const double xm = i == 0 ? xl : x64[i - 1];
-        const double xp = i == M - 1 ? xr : x64[i + 1];
-        double r = d64[i] - (double)wb[i] * x64[i];
-        r = fma(-(double)wa[i], xm, r);
-        r = fma(-(double)wc[i], xp, r);
-        wd[i] = (float)r;
-      }
+      const float r = rcp_fast(wb[i] - wa[i] * wc[i - 1]);
+      psum += fabsf(r);
+      rr[i] = r;
+      wd[i] = r * (wd[i] - wa[i] * wd[i - 1]);
+      wa[i] = -r * wa[i] * wa[i - 1];
+      wc[i] = r * wc[i];
     }
-    fp32_chunk_solve<M>(wa, wb, wc, wd, lane, 32, bad);
-    double dmax = 0.0, xmax = 0.0;
+  }
+  sts_swz<float, M>(tr, lane, rr);
+  sts_swz<float, M>(tfa, lane, wa);
+  // backward recursion (matrix part once, right-hand side each pass)
+  float A = wa[M - 2], C = wc[M - 2], Dd = wd[M - 2];
+#pragma unroll
+  for (int j = M - 3; j >= 1; --j) {
+    Dd = wd[j] - wc[j] * Dd;
+    A = wa[j] - wc[j] * A;
+    C = -wc[j] * C;
+  }
+  const float r0 = rcp_fast(1.f - wc[0] * A);
+  psum += fabsf(r0);
+  const float c0 = wc[0];
+  const float tA = r0 * wa[0], tC = -r0 * c0 * C;
+  const float bA = wa[M - 1], bC = wc[M - 1];
+  // reduced system: form it, recording the PCR coefficients of every level
+  constexpr int L = 5;  // log2(32)
+  float cal[L], cga[L], crl[L];
+  float rbe;
+  float y, z;
+  {
+    float pA = __shfl_up_sync(FULL_MASK, bA, 1), pC = __shfl_up_sync(FULL_MASK, bC, 1);
+    if (lane == 0) pA = pC = 0.f;
+    float al = -tA * pA;
+    const float be = 1.f - tA * pC - tC * bA;
+    float ga = -tC * bC;
+    rbe = rcp_fast(be);
+    psum += fabsf(rbe);
+    al *= rbe;
+    ga *= rbe;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const int sft = 1 << l;
+      float al_l = __shfl_up_sync(FULL_MASK, al, sft), ga_l = __shfl_up_sync(FULL_MASK, ga, sft);
+      float al_r = __shfl_down_sync(FULL_MASK, al, sft), ga_r = __shfl_down_sync(FULL_MASK, ga, sft);
+      if (lane < sft) al_l = ga_l = 0.f;
+      if (lane + sft >= 32) al_r = ga_r = 0.f;
+      const float r = rcp_fast(1.f - al * ga_l - ga * al_r);
+      psum += fabsf(r);
+      cal[l] = al;
+      cga[l] = ga;
+      crl[l] = r;
+      al = -al * al_l * r;
+      ga = -ga * ga_r * r;
+    }
+  }
+  // right-hand-side part of the reduced solve and the back-substitution,
+  // shared by every pass; wd holds d' (forward-eliminated right-hand side)
+  auto finish = [&](const float (&fa)[M], const float (&fc)[M], float topD, float (&dx)[M]) {
+    const float botD = wd[M - 1];
+    float pD = __shfl_up_sync(FULL_MASK, botD, 1);
+    if (lane == 0) pD = 0.f;
+    float de = (topD - tA * pD - tC * botD) * rbe;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const int sft = 1 << l;
+      float de_l = __shfl_up_sync(FULL_MASK, de, sft);
+      float de_r = __shfl_down_sync(FULL_MASK, de, sft);
+      if (lane < sft) de_l = 0.f;
+      if (lane + sft >= 32) de_r = 0.f;
+      de = (de - cal[l] * de_l - cga[l] * de_r) * crl[l];
+    }
+    y = de;
+    float yn = __shfl_down_sync(FULL_MASK, y, 1);
+    if (lane == 31) yn = 0.f;
+    z = botD - bA * y - bC * yn;
+    float x = z;
+    dx[M - 1] = z;
+#pragma unroll
+    for (int j = M - 2; j >= 1; --j) {
+      x = wd[j] - fa[j] * y - fc[j] * x;
+      dx[j] = x;
+    }
+    dx[0] = y;
+  };
+  bad |= !(psum <= 3.4e38f);
+  double x64[M];
+  {
+    float dx[M];
+    finish(wa, wc, r0 * (wd[0] - c0 * Dd), dx);
+#pragma unroll
+    for (int i = 0; i < M; ++i) x64[i] = (double)dx[i];
+  }
+  // max|dx| of this pass, and the estimated relative error of x after it
+  float dprev = 0.f;
+  auto converged = [&](const float (&dx)[M], double &est) {
+    float dmax = 0.f;
+    double xm64 = 0.0;
 #pragma unroll
     for (int i = 0; i < M; ++i) {
-      x64[i] += (double)wd[i];
-      dmax = fmax(dmax, fabs((double)wd[i]));
-      xmax = fmax(xmax, fabs(x64[i]));
+      dmax = fmaxf(dmax, fabsf(dx[i]));
+      xm64 = fmax(xm64, fabs(x64[i]));
     }
+    float xmax = (float)fmin(xm64, 3.0e38);  // a norm for the stopping test: FP32 is plenty
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      dmax = fmax(dmax, __shfl_xor_sync(FULL_MASK, dmax, o));
-      xmax = fmax(xmax, __shfl_xor_sync(FULL_MASK, xmax, o));
+      dmax = fmaxf(dmax, __shfl_xor_sync(FULL_MASK, dmax, o));
+      xmax = fmaxf(xmax, __shfl_xor_sync(FULL_MASK, xmax, o));
     }
-    ++it;
-    rel = xmax > 0.0 ? dmax / xmax : 0.0;
-    if (!(rel > p.tol) || it >= p.max_iters) break;  // uniform across the warp
-  }
-  // x out through the FP64 tile (own row), then coalesced 16-byte stores
+    est = mixed_error_estimate(dmax, dprev, (double)xmax);
+    dprev = dmax;
+  };
+  int it = 1;
+  double rel = 0.0;
+  {
+    // the first correction is x itself
+    float dx0[M];
 #pragma unroll
-  for (int i = 0; i < M; ++i) td[lane * RD + i] = x64[i];
+    for (int i = 0; i < M; ++i) dx0[i] = (float)x64[i];
+    converged(dx0, rel);
+  }
+
+  // ---- refinement passes
+  while (rel > p.tol && it < p.max_iters) {  // uniform across the warp
+    // FP64 residual r = d - T x, rounded to FP32, and the forward sweep
+    double xl = __shfl_up_sync(FULL_MASK, x64[M - 1], 1);
+    double xr = __shfl_down_sync(FULL_MASK, x64[0], 1);
+    if (lane == 0) xl = 0.0;
+    if (lane == 31) xr = 0.0;
+#pragma unroll
+    for (int q = 0; q < M / 4; ++q) {
+      const float4 a4 = *reinterpret_cast<const float4 *>(ta + SF::unit(lane, q));
+      const float4 b4 = *reinterpret_cast<const float4 *>(tb + SF::unit(lane, q));
+      const float4 c4 = *reinterpret_cast<const float4 *>(tc + SF::unit(lane, q));
+      const float4 r4 = *reinterpret_cast<const float4 *>(tr + SF::unit(lane, q));
+      const double2 d01 = *reinterpret_cast<const double2 *>(td + SD::unit(lane, 2 * q));
+      const double2 d23 = *reinterpret_cast<const double2 *>(td + SD::unit(lane, 2 * q + 1));
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
+      const float cv[4] = {c4.x, c4.y, c4.z, c4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+      const double dv[4] = {d01.x, d01.y, d23.x, d23.y};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = 4 * q + k;
+        const double xm = i == 0 ? xl : x64[i - 1];
+        const double xp = i == M - 1 ? xr : x64[i + 1];
+        double res = dv[k] - (double)bv[k] * x64[i];
+        res = fma(-(double)av[k], xm, res);
+        res = fma(-(double)cv[k], xp, res);
+        const float rf = (float)res;
+        wd[i] = i < 2 ? rv[k] * rf : rv[k] * (rf - av[k] * wd[i - 1]);
+      }
+    }
+    float fa[M], fc[M], rr2[M];
+    lds_swz<float, M>(tfa, lane, fa);
+    lds_swz<float, M>(tr, lane, rr2);
+    lds_swz<float, M>(tc, lane, fc);
+#pragma unroll
+    for (int j = 0; j < M; ++j) fc[j] *= rr2[j];
+    float D2 = wd[M - 2];
+#pragma unroll
+    for (int j = M - 3; j >= 1; --j) D2 = wd[j] - fc[j] * D2;
+    float dx[M];
+    finish(fa, fc, r0 * (wd[0] - c0 * D2), dx);
+#pragma unroll
+    for (int i = 0; i < M; ++i) x64[i] += (double)dx[i];
+    converged(dx, rel);
+    ++it;
+  }
+
+  // x out through the FP64 tile (own row), then coalesced 16-byte stores
+  sts_swz<double, M>(td, lane, x64);
   __syncwarp();
-  const int nud = (N + 1) / 2;
-  for (int un = lane; un < nud; un += 32) {
-    const int e = un * 2;
-    const double2 v = *reinterpret_cast<const double2 *>(td + e + (e / M) * 2);
-    if (e + 2 <= N) {
-      *reinterpret_cast<double2 *>(p.d + base + e) = v;
-    } else {
-      p.d[base + e] = v.x;
+  if (full) {
+#pragma unroll
+    for (int k = 0; k < M / 2; ++k) {
+      const int e = 2 * (lane + 32 * k);
+      *reinterpret_cast<double2 *>(p.d + base + e) = *reinterpret_cast<const double2 *>(td + SD::off(e));
+    }
+  } else {
+    const int nud = (N + 1) / 2;
+    for (int un = lane; un < nud; un += 32) {
+      const int e = un * 2;
+      const double2 v = *reinterpret_cast<const double2 *>(td + SD::off(e));
+      if (e + 2 <= N) {
+        *reinterpret_cast<double2 *>(p.d + base + e) = v;
+      } else {
+        p.d[base + e] = v.x;
+      }
     }
   }
   if (lane == 0) mixed_report(it, rel);
@@ -211,7 +477,8 @@ __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
   double *cd = xl + TW;                                // max |dx| of chunk (t, s)
   double *cx = cd + TW;                                // max |x| of chunk (t, s)
   double *relv = cx + TW;                              // per system
-  int *conv = reinterpret_cast<int *>(relv + W);
+  double *dpv = relv + W;                              // previous max |dx|, per system
+  int *conv = reinterpret_cast<int *>(dpv + W);
   float *red = reinterpret_cast<float *>(conv + W + (W & 1));
   const int tid = threadIdx.x;
   const int s = tid % W;
@@ -295,7 +562,8 @@ __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
         dm = fmax(dm, cd[q * W + s]);
         xm = fmax(xm, cx[q * W + s]);
       }
-      const double rel = xm > 0.0 ? dm / xm : 0.0;
+      const double rel = mixed_error_estimate((float)dm, it == 0 ? 0.f : (float)dpv[s], xm);
+      dpv[s] = dm;
       relv[s] = rel;
       conv[s] = !(rel > p.tol);
     }
@@ -323,10 +591,12 @@ static int pow2c(long long v) {
   return q;
 }
 
+// One warp per CTA: ~20 KB of shared memory per system, so up to 11 warps
+// per SM; larger CTAs would round the shared-memory use up.
 template <int M>
 static cudaError_t launch_mixed_contig(const MixedArgs &p, cudaStream_t st) {
-  const int threads = 128;
-  const size_t per_warp = (size_t)3 * 32 * (M + 4) * 4 + (size_t)32 * (M + 2) * 8;
+  const int threads = 32;
+  const size_t per_warp = (size_t)5 * 32 * M * 4 + (size_t)32 * M * 8;
   const size_t smem = per_warp * (threads / 32);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(mixed_contig_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -340,7 +610,7 @@ template <int M, int KR>
 static cudaError_t launch_mixed_strided(const MixedArgs &p, int T, int W, cudaStream_t st) {
   const long long ngx = (p.n0 + W - 1) / W;
   const long long blocks = ngx * (p.nsys / p.n0);
-  const size_t smem = (size_t)(4 * T * W + W) * 8 + (size_t)(W + (W & 1)) * 4 +
+  const size_t smem = (size_t)(4 * T * W + 2 * W) * 8 + (size_t)(W + (W & 1)) * 4 +
                       (size_t)6 * T * (W + 1) * 4;
   mixed_strided_kernel<M, KR><<<(unsigned)blocks, W * T, smem, st>>>(p, T, W, ngx);
   g_launches.fetch_add(1, std::memory_order_relaxed);

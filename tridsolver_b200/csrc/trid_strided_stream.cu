@@ -28,8 +28,9 @@
 //   4. after the block-wide reduced solve, back-substitutes
 //          x_i = d'_i - a'_i x_first - c'_i x_{i+1}
 //      from the chunk's last row up, and stores.
-// Inc variants read u after the reduced solve, so its latency overlaps the
-// back-substitution. Every element is read once and written once.
+// Inc variants carry u through the same window and park it in a third set
+// of private slots until the store. Every element is read once and written
+// once.
 #include <cuda_runtime.h>
 
 #include "trid_internal.h"
@@ -42,20 +43,22 @@ template <typename R> constexpr int stream_w() { return 128 / (int)sizeof(R); }
 template <typename R> constexpr int stream_bs() { return 32 * stream_w<R>(); }
 
 // Row `row` at element offset o: identity rows outside the system, a[0] and
-// c[N-1] forced to zero.
-template <typename R>
+// c[N-1] forced to zero; u too for Inc.
+template <typename R, bool INC>
 __device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, long long o, bool valid,
-                                                int row, R &a, R &b, R &c, R &d) {
+                                                int row, R &a, R &b, R &c, R &d, R &u) {
   if (valid) {
     a = row == 0 ? R(0) : __ldg(p.a + o);
     b = __ldg(p.b + o);
     c = row == p.N - 1 ? R(0) : __ldg(p.c + o);
     d = __ldg(p.d_in + o);
+    if constexpr (INC) u = __ldg(p.u + o);
   } else {
     a = R(0);
     b = R(1);
     c = R(0);
     d = R(0);
+    if constexpr (INC) u = R(0);
   }
 }
 
@@ -76,6 +79,7 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
   R *saf = red + RED + tid;             // a' of row j at [j * BS]
   R *scf = red + RED + M * BS + tid;    // c'
   R *sdf = red + RED + 2 * M * BS + tid;  // d' (SD)
+  R *suf = red + RED + (SD ? 3 : 2) * M * BS + tid;  // u (Inc)
   const int s = tid % W;
   const int t = tid / W;
   const int N = p.N;
@@ -91,13 +95,15 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
   };
 
-  // L2 prefetch lanes (PF > 0): lane l < 16 covers one end (first or last
-  // system) of the row segment of one array for one of the warp's two chunks
+  // L2 prefetch lanes (PF > 0): lane l < 2 * NA * (32 / W) covers one end
+  // (first or last system) of the row segment of one of the NA arrays for
+  // one of the warp's chunks
+  constexpr int NA = INC ? 5 : 4;
   const int lane = tid & 31;
-  const bool pf_lane = PF > 0 && lane < 16;
-  const int pq = (lane >> 1) & 3;
-  const int pt = (tid >> 5) * (32 / W) + (lane >> 3);
-  const R *pbase = pq == 0 ? p.a : pq == 1 ? p.b : pq == 2 ? p.c : p.d_in;
+  const bool pf_lane = PF > 0 && lane < 2 * NA * (32 / W);
+  const int pq = (lane >> 1) % NA;
+  const int pt = (tid >> 5) * (32 / W) + (lane >> 1) / NA;
+  const R *pbase = pq == 0 ? p.a : pq == 1 ? p.b : pq == 2 ? p.c : pq == 3 ? p.d_in : p.u;
   auto pf_first = [&](long long g, bool &ok) -> long long {
     const long long gx = g % ngx;
     const long long i1 = g / ngx;
@@ -107,14 +113,15 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     return ok ? i0 * p.st0 + i1 * p.st1 + (long long)pt * M * stride : 0;
   };
 
-  R pa[D], pb[D], pc[D], pd[D];
+  R pa[D], pb[D], pc[D], pd[D], pu[INC ? D : 1];
   long long g = blockIdx.x;
   bool act;
   long long first = group_first(g, act);
   long long lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    stream_load_row<R>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
+    stream_load_row<R, INC>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j],
+                            pu[INC ? j : 0]);
     lo += stride;
   }
   bool pok = false;
@@ -137,13 +144,14 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     for (int j = 0; j < M; ++j) {
       const int k = j % D;
       const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
+      if constexpr (INC) suf[j * BS] = pu[k];
       if (j + D < M) {
         const int row = row0 + j + D;
-        stream_load_row<R>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        stream_load_row<R, INC>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k], pu[INC ? k : 0]);
         lo += stride;
       } else {
         const int row = row0 + j + D - M;
-        stream_load_row<R>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        stream_load_row<R, INC>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k], pu[INC ? k : 0]);
         ln += stride;
       }
       if constexpr (PF > 0) {
@@ -204,17 +212,6 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     R y, z;
     block_reduced_solve<R, 2>(red, top, bot, s, t, T, W, y, z, bad);
 
-    // Inc: u is read now, its latency overlapping the back-substitution
-    R uu[INC ? M : 1];
-    if constexpr (INC) {
-      long long o = first;
-#pragma unroll
-      for (int j = 0; j < M; ++j) {
-        uu[j] = (act && row0 + j < N) ? __ldg(p.u + o) : R(0);
-        o += stride;
-      }
-    }
-
     // back-substitution with the forward rows, stored as it goes (last row
     // first)
     long long o = first + (long long)(M - 1) * stride;
@@ -224,7 +221,7 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
       if (j < M - 1) x = j == 0 ? y : dval(j) - saf[j * BS] * y - scf[j * BS] * x;
       if (act && row0 + j < N) {
         if constexpr (INC)
-          p.u[o] = uu[j] + x;
+          p.u[o] = suf[j * BS] + x;
         else
           p.d_out[o] = x;
       }
@@ -268,7 +265,7 @@ static cudaError_t launch_stream_pf(const BatchArgs<R> &p, cudaStream_t st) {
   constexpr int D = stream_window<R, M>();
   constexpr bool SD = stream_sd<R, M>();
   const size_t red = ((size_t)6 * 32 * (W + 1) * sizeof(R) + 15) / 16 * 16;
-  const size_t smem = red + (size_t)(SD ? 3 : 2) * M * BS * sizeof(R);
+  const size_t smem = red + (size_t)(2 + (SD ? 1 : 0) + (INC ? 1 : 0)) * M * BS * sizeof(R);
   auto kern = strided_stream_kernel<R, M, D, SD, PF, INC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
