@@ -80,12 +80,16 @@ EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *
 EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a, const float *b,
                                            const float *c, float *d, const int64_t *offsets,
                                            long long nsys);
-/* Times every rows-per-lane choice per length class on this device (uniform
- * synthetic batches, about a second) and keeps the fastest for later ragged
- * calls of that precision on the current device. */
+/* Times, per length class up to one warp's worth of rows, every
+ * rows-per-lane choice of a warp per system and the staged 512-row tile
+ * path, on this device (uniform synthetic batches, about a second), and
+ * keeps the fastest for later ragged calls of that precision on the current
+ * device. Longer systems always take 512-row tiles (up to 32 per system,
+ * N <= 16384). */
 EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
-/* Copies the rows-per-lane table in use (one entry per length class
- * ceil(log2 N) = 0, 1, ...) and returns the number of classes, or -1. */
+/* Copies the table in use (one entry per length class ceil(log2 N) = 0, 1,
+ * ...: rows per lane of a warp per system, or 0 for 512-row tiles) and
+ * returns the number of classes, or -1. */
 EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses);
 
 /* ---- ADI heat-diffusion timestep -----------------------------------------

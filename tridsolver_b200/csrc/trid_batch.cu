@@ -258,7 +258,7 @@ static cudaError_t launch_long_m(const BatchArgs<R> &p, cudaStream_t st) {
   if (2 * nc >= p.N) return cudaErrorInvalidValue;  // would not shrink
   const long long nred = p.nsys * 2 * nc;
   R *scratch = nullptr;
-  cudaError_t e = cudaMallocAsync((void **)&scratch, (size_t)nred * 4 * sizeof(R), st);
+  cudaError_t e = scratch_alloc((void **)&scratch, (size_t)nred * 4 * sizeof(R), st);
   if (e != cudaSuccess) return e;
   R *ra = scratch, *rb = ra + nred, *rc = rb + nred, *rd = rc + nred;
   const int threads = 128;
@@ -292,7 +292,7 @@ static cudaError_t launch_long_m(const BatchArgs<R> &p, cudaStream_t st) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
   }
-  cudaError_t ef = cudaFreeAsync(scratch, st);
+  cudaError_t ef = scratch_free(scratch, st);
   return e != cudaSuccess ? e : ef;
 }
 

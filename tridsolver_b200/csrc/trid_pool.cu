@@ -1,0 +1,62 @@
+// Scratch memory of the library: stream-ordered allocations from a pool that
+// the library owns, one per device, which keeps its memory between calls
+// (release threshold: unlimited). With the device's default pool (release
+// threshold 0) every synchronisation hands the scratch back to the driver
+// and the next call maps it again: measured at about 1.1 ms per ragged call
+// of 200,000 systems. The default pool of the process is left untouched.
+// While a stream is being captured into a CUDA graph the default pool is
+// used, so the allocation becomes a graph memory node as usual.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "trid_internal.h"
+
+namespace trid {
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+}  // namespace
+
+static cudaMemPool_t library_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t st) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
+  }
+  cudaMemPool_t pool = cap == cudaStreamCaptureStatusNone ? library_pool() : nullptr;
+  if (pool) return cudaMallocFromPoolAsync(ptr, bytes, pool, st);
+  return cudaMallocAsync(ptr, bytes, st);
+}
+
+cudaError_t scratch_free(void *ptr, cudaStream_t st) { return cudaFreeAsync(ptr, st); }
+
+}  // namespace trid

@@ -3,23 +3,31 @@
 // persistent launch.
 //
 //   1. ragged_hist_kernel / ragged_order_kernel bucket the systems by length
-//      class (ceil(log2 N)) into `order`, longest class first, so the
-//      persistent kernel hands out the longest work first (longest-processing
-//      -time scheduling keeps the SMs evenly loaded at the end);
-//   2. ragged_kernel: persistent CTAs of 256 threads. Phase 1 takes "block
-//      items" (systems longer than one warp holds) one per CTA, from a
-//      global atomic counter; phase 2 takes "warp items", one system per warp,
-//      each warp on its own.
+//      class (ceil(log2 N)), longest class first (longest-processing-time
+//      order keeps the SMs evenly loaded at the end). A system of a "tile"
+//      class is cut into K = ceil(N / 512) tiles of 512 rows and each tile
+//      becomes one work item; a system of a "warp" class (short systems,
+//      rows-per-lane M from the class table) is one warp item;
+//   2. ragged_kernel: persistent warps take tile items (longest systems
+//      first), then warp items, from one global counter.
 //
-// Warp items run the partition hybrid over 32 lanes with M rows per lane
-// chosen per length class from a table (M = 1 is pure PCR, one row per
-// lane); the table is built in, or measured by tridRaggedAutotune.
-// Block items (N up to 16384): 256 threads x 16 rows = one 4096-row segment
-// per pass. Pass A eliminates every segment's chunks and keeps only their
-// reduced rows in shared memory; the CTA solves that reduced system (each
-// thread eliminates its 2*nseg consecutive reduced rows, then the block
-// reduced solve); pass B reads each segment again (mostly from L2, the CTA
-// read it moments before), eliminates it again and substitutes.
+// Tile item (one warp, 16 rows per lane): the warp stages the tile's rows of
+// a, b, c, d in shared memory with coalesced cp.async copies, each lane runs
+// the chunk elimination on its 16 rows, and the warp's reduced solve is run
+// for three right-hand sides at once: the tile's own, and the unit
+// couplings to the unknown just before the tile (x_prev, the previous
+// tile's last) and just after it (x_next, the next tile's first). Every
+// reduced unknown of the tile is then p + alpha x_prev + beta x_next. From
+// the tile's first and last unknowns the warp forms the tile's two rows of
+// a second-level tridiagonal system (2 rows per tile, at most 64 rows), and
+// the warp that finishes the last tile of a system solves it with one warp
+// PCR and publishes every tile's first and last unknown. The other warps of
+// the system wait for that (a bounded wait on a flag) while keeping their
+// tile in registers, then substitute and store. So every element is read
+// once and written once, with 8 values of scratch per tile. Claims are in
+// system order, so the tiles a warp waits for are held by running warps:
+// the wait always ends.
+//
 // The reference has no ragged entry point; its per-system solve trid_scalar
 // (scalar/src/cpu/trid_cpu.cpp:312-353) is the oracle for each system.
 #include <cuda_runtime.h>
@@ -31,24 +39,33 @@
 
 namespace trid {
 
-constexpr int kClasses = 24;          // length classes 0..23: N <= 2^class
-constexpr int kBlockThreads = 256;
-constexpr int kBlockM = 16;           // rows per thread in block items
-constexpr int kSegRows = kBlockThreads * kBlockM;  // 4096
-constexpr int kMaxSeg = 4;            // block items up to 16384 rows
+constexpr int kClasses = 24;        // length classes 0..23: N <= 2^class
+constexpr int kTM = 16;             // rows per lane in tile items
+constexpr int kTileRows = 32 * kTM; // 512
+constexpr int kMaxTiles = 32;       // tiles per system: N <= 16384
+constexpr int kRaggedThreads = 128; // 4 warps per CTA
+constexpr unsigned kWaitLimit = 1u << 22;  // polls of the ready flag (each with a short sleep)
 
 template <typename R> struct RaggedArgs {
   const R *a, *b, *c;
   R *d;
   const int64_t *off;
-  const int *order;                 // systems, longest class first
+  const int *order;                 // warp-item systems, longest class first
   const unsigned *hist;             // systems per class
-  unsigned long long *counters;     // [0] block items taken, [1] warp items taken
+  const unsigned long long *tiles;  // tiles per class (tile classes)
+  const int *tile_sys;              // system of each tile item
+  const long long *tstart;          // first tile item of each (tile-class) system
+  R *tile_rows;                     // 6 per tile: top A, C, D; bottom A, C, D
+  R *tile_fl;                       // 2 per tile: first and last unknown
+  unsigned *sys_done;               // tiles of the system past the reduction
+  unsigned *sys_ready;              // second-level solution published
+  unsigned long long *counter;      // work items taken
   long long nsys;
-  int warp_max;                     // longest system a warp item takes
-  int mtab[kClasses];               // rows per lane by class (warp items)
+  int mtab[kClasses];               // rows per lane by class; 0 = tile class
   unsigned *flag;
-  unsigned *error;                  // set when a system exceeds the block-item limit
+  unsigned *error;                  // 1: a system longer than 16384 rows; 2: a wait gave up;
+                                    // 3: the tile table was too small
+  long long max_tiles;              // entries of tile_sys / tile_rows / tile_fl
 };
 
 __device__ __forceinline__ int length_class(long long n) {
@@ -58,24 +75,43 @@ __device__ __forceinline__ int length_class(long long n) {
 }
 
 template <typename R>
-__global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist) {
-  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < p.nsys;
-       s += (long long)gridDim.x * blockDim.x) {
-    const long long n = p.off[s + 1] - p.off[s];
-    atomicAdd(&hist[length_class(n > 0 ? n : 1)], 1u);
-  }
-}
-
-template <typename R>
-__global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist, unsigned *fill,
-                                    int *order) {
+__global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist, unsigned long long *tiles) {
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < p.nsys;
        s += (long long)gridDim.x * blockDim.x) {
     const long long n = p.off[s + 1] - p.off[s];
     const int c = length_class(n > 0 ? n : 1);
-    unsigned start = 0;
-    for (int q = kClasses - 1; q > c; --q) start += hist[q];
-    order[start + atomicAdd(&fill[c], 1u)] = (int)s;
+    atomicAdd(&hist[c], 1u);
+    if (p.mtab[c] == 0) atomicAdd(&tiles[c], (unsigned long long)((n + kTileRows - 1) / kTileRows));
+  }
+}
+
+template <typename R>
+__global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist,
+                                    const unsigned long long *tiles, unsigned *fill,
+                                    unsigned long long *tfill, int *order, int *tile_sys,
+                                    long long *tstart) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < p.nsys;
+       s += (long long)gridDim.x * blockDim.x) {
+    const long long n = p.off[s + 1] - p.off[s];
+    const int c = length_class(n > 0 ? n : 1);
+    if (p.mtab[c] == 0) {
+      unsigned long long t0 = 0;
+      for (int q = kClasses - 1; q > c; --q)
+        if (p.mtab[q] == 0) t0 += tiles[q];
+      const long long K = (n + kTileRows - 1) / kTileRows;
+      const long long ts = (long long)(t0 + atomicAdd(&tfill[c], (unsigned long long)K));
+      tstart[s] = ts;
+      if (ts + K > p.max_tiles) {  // offsets not ascending: refuse rather than overrun
+        atomicExch(p.error, 3u);
+        continue;
+      }
+      for (long long j = 0; j < K; ++j) tile_sys[ts + j] = (int)s;
+    } else {
+      unsigned start = 0;
+      for (int q = kClasses - 1; q > c; --q)
+        if (p.mtab[q] != 0) start += hist[q];
+      order[start + atomicAdd(&fill[c], 1u)] = (int)s;
+    }
   }
 }
 
@@ -102,71 +138,7 @@ __device__ __forceinline__ void ragged_load(const RaggedArgs<R> &p, long long ba
   }
 }
 
-template <typename R, int M>
-__device__ __forceinline__ void ragged_store(const RaggedArgs<R> &p, long long base, long long n,
-                                             long long row0, const R (&x)[M]) {
-#pragma unroll
-  for (int i = 0; i < M; ++i)
-    if (row0 + i < n) p.d[base + row0 + i] = x[i];
-}
-
-// Segment staging for block items: the CTA copies rows [row0, row0+kSegRows)
-// of a, b, c, d into shared memory with element-sized cp.async copies, so
-// every warp instruction copies 32 consecutive elements (offsets need not be
-// aligned). Thread t's chunk (rows t*kBlockM ...) sits in a row padded by one
-// element, so its reads of neighbouring threads fall in different banks.
-constexpr int kStageRow = kBlockM + 1;
-constexpr int kStageArr = kBlockThreads * kStageRow;
-
-__device__ __forceinline__ void cp_async_elem(void *smem_dst, const void *gmem_src, int bytes) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  if (bytes == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
-
-template <typename R>
-__device__ __forceinline__ void stage_segment(const RaggedArgs<R> &p, long long base, long long n,
-                                              long long row0, R *stg) {
-  for (int e = threadIdx.x; e < kSegRows; e += kBlockThreads) {
-    const long long row = row0 + e;
-    const int o = e + e / kBlockM;
-    if (row < n) {
-      cp_async_elem(stg + 0 * kStageArr + o, p.a + base + row, (int)sizeof(R));
-      cp_async_elem(stg + 1 * kStageArr + o, p.b + base + row, (int)sizeof(R));
-      cp_async_elem(stg + 2 * kStageArr + o, p.c + base + row, (int)sizeof(R));
-      cp_async_elem(stg + 3 * kStageArr + o, p.d + base + row, (int)sizeof(R));
-    } else {
-      stg[0 * kStageArr + o] = R(0);
-      stg[1 * kStageArr + o] = R(1);
-      stg[2 * kStageArr + o] = R(0);
-      stg[3 * kStageArr + o] = R(0);
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-}
-
-// Thread t's kBlockM rows of a staged segment, a[0] and c[n-1] zero.
-template <typename R>
-__device__ __forceinline__ void staged_rows(const R *stg, long long n, long long row0, R (&a)[kBlockM],
-                                            R (&b)[kBlockM], R (&c)[kBlockM], R (&d)[kBlockM]) {
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int i = 0; i < kBlockM; ++i) {
-    const int o = t * kStageRow + i;
-    a[i] = stg[0 * kStageArr + o];
-    b[i] = stg[1 * kStageArr + o];
-    c[i] = stg[2 * kStageArr + o];
-    d[i] = stg[3 * kStageArr + o];
-    const long long row = row0 + t * kBlockM + i;
-    if (row == 0) a[i] = R(0);
-    if (row == n - 1) c[i] = R(0);
-  }
-}
-
-// One system per warp, M rows per lane (M = 1: pure PCR).
+// One short system per warp, M rows per lane (M = 1: pure PCR).
 template <typename R, int M>
 __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base, long long n,
                                           int lane, bool &bad) {
@@ -189,163 +161,278 @@ __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base
     reduced_solve<R>(Row<R>{a[0], c[0], d[0]}, Row<R>{a[M - 1], c[M - 1], d[M - 1]}, lane, 32, y, z,
                      bad);
     chunk_substitute<R, M>(a, c, d, y, z);
-    ragged_store<R, M>(p, base, n, (long long)lane * M, d);
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+      if ((long long)lane * M + i < n) p.d[base + (long long)lane * M + i] = d[i];
   }
 }
 
-// One long system per CTA (kBlockThreads threads, NS padded segments).
-template <typename R, int NS>
-__device__ __forceinline__ void block_item_ns(const RaggedArgs<R> &p, long long base, long long n,
-                                              R *sm_red, R *sm_bs, R *stg, bool &bad) {
-  const int t = threadIdx.x;
-  const int Q = kBlockThreads * NS;  // chunks of the system (padded)
-  // pass A: per segment, chunk elimination; keep the two reduced rows
-  for (int g = 0; g < NS; ++g) {
-    R a[kBlockM], b[kBlockM], c[kBlockM], d[kBlockM];
-    if ((long long)g * kSegRows < n) {
-      stage_segment<R>(p, base, n, (long long)g * kSegRows, stg);
-      staged_rows<R>(stg, n, (long long)g * kSegRows, a, b, c, d);
-      __syncthreads();  // the staging buffer is free again
+// The warp's reduced solve (as reduced_solve, 32 lanes) for three
+// right-hand sides sharing the matrix: k = 0 the rows' own D; k = 1 only
+// tD1 on the top row (lane 0: the coupling to the unknown before the
+// tile); k = 2 only bD2 on the bottom row (lane 31: the coupling to the one
+// after it).
+template <typename R>
+__device__ __forceinline__ void reduced_solve3(const Row<R> &top, const Row<R> &bot, R tD1, R bD2,
+                                               int t, R (&y)[3], R (&z)[3], bool &bad) {
+  constexpr int T = 32;
+  const R tD[3] = {top.D, tD1, R(0)};
+  const R bD[3] = {bot.D, R(0), bD2};
+  R pA = shfl_up(bot.A, 1, T), pC = shfl_up(bot.C, 1, T);
+  R de[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    R pD = shfl_up(bD[k], 1, T);
+    if (t == 0) pD = R(0);
+    de[k] = tD[k] - top.C * bD[k];
+    de[k] -= top.A * pD;
+  }
+  if (t == 0) {
+    pA = R(0);
+    pC = R(0);
+  }
+  R al = -top.A * pA;
+  const R be = R(1) - top.A * pC - top.C * bot.A;
+  R ga = -top.C * bot.C;
+  R r = rcp(be);
+  bad |= !finite_rcp(r);
+  al *= r;
+  ga *= r;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) de[k] *= r;
+#pragma unroll
+  for (int s = 1; s < T; s <<= 1) {
+    R al_l = shfl_up(al, s, T), ga_l = shfl_up(ga, s, T);
+    R al_r = shfl_down(al, s, T), ga_r = shfl_down(ga, s, T);
+    R dl[3], dr[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      dl[k] = shfl_up(de[k], s, T);
+      dr[k] = shfl_down(de[k], s, T);
+    }
+    if (t < s) {
+      al_l = ga_l = R(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) dl[k] = R(0);
+    }
+    if (t + s >= T) {
+      al_r = ga_r = R(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) dr[k] = R(0);
+    }
+    r = rcp(R(1) - al * ga_l - ga * al_r);
+    bad |= !finite_rcp(r);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) de[k] = (de[k] - al * dl[k] - ga * dr[k]) * r;
+    al = -al * al_l * r;
+    ga = -ga * ga_r * r;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    y[k] = de[k];
+    R yn = shfl_down(y[k], 1, T);
+    if (t == T - 1) yn = R(0);
+    z[k] = bD[k] - bot.A * y[k] - bot.C * yn;
+  }
+}
+
+// Shared memory of one warp's tile: a, b, c, d in padded chunk rows (as
+// contig_smem_kernel), d's rows reused for x on the way out.
+template <typename R> struct TileBuf {
+  using L = SmemLayout<R, kTM>;
+  static constexpr int ELEMS = 4 * L::BUF;
+  __device__ static __forceinline__ int slot(int e) { return (e / kTM) * L::ROW + e % kTM; }
+};
+
+// Copies rows [0, nt) of the tile starting at element `base` into the warp's
+// buffer (element-sized cp.async: 32 consecutive elements per instruction,
+// any alignment); rows nt..511 become identity rows.
+template <typename R>
+__device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long base, int nt, R *buf,
+                                           int lane) {
+  using L = SmemLayout<R, kTM>;
+#pragma unroll 4
+  for (int e = lane; e < kTileRows; e += 32) {
+    const int o = TileBuf<R>::slot(e);
+    if (e < nt) {
+      cp_async_elem<R>(buf + 0 * L::BUF + o, p.a + base + e);
+      cp_async_elem<R>(buf + 1 * L::BUF + o, p.b + base + e);
+      cp_async_elem<R>(buf + 2 * L::BUF + o, p.c + base + e);
+      cp_async_elem<R>(buf + 3 * L::BUF + o, p.d + base + e);
     } else {
+      buf[0 * L::BUF + o] = R(0);
+      buf[1 * L::BUF + o] = R(1);
+      buf[2 * L::BUF + o] = R(0);
+      buf[3 * L::BUF + o] = R(0);
+    }
+  }
+  cp_async_wait_all();
+  __syncwarp();
+}
+
+template <typename R>
+__device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item, R *buf, int lane,
+                                          bool &bad) {
+  using L = SmemLayout<R, kTM>;
+  const int s = p.tile_sys[item];
+  const long long ts = p.tstart[s];
+  const int j = (int)(item - ts);
+  const long long base0 = p.off[s];
+  const long long n = p.off[s + 1] - base0;
+  const int K = (int)((n + kTileRows - 1) / kTileRows);
+  const long long r0 = (long long)j * kTileRows;
+  const int nt = (int)(n - r0 < kTileRows ? n - r0 : kTileRows);
+  stage_tile<R>(p, base0 + r0, nt, buf, lane);
+
+  R a[kTM], b[kTM], c[kTM], d[kTM];
+  lds_row<R, kTM>(buf + 0 * L::BUF + lane * L::ROW, a);
+  lds_row<R, kTM>(buf + 1 * L::BUF + lane * L::ROW, b);
+  lds_row<R, kTM>(buf + 2 * L::BUF + lane * L::ROW, c);
+  lds_row<R, kTM>(buf + 3 * L::BUF + lane * L::ROW, d);
+  const long long row0 = r0 + (long long)lane * kTM;
+  if (row0 == 0) a[0] = R(0);
 #pragma unroll
-      for (int i = 0; i < kBlockM; ++i) {
-        a[i] = R(0);
-        b[i] = R(1);
-        c[i] = R(0);
-        d[i] = R(0);
+  for (int i = 0; i < kTM; ++i)
+    if (row0 + i == n - 1) c[i] = R(0);
+  chunk_forward<R, kTM>(a, b, c, d, bad);
+  chunk_backward<R, kTM>(a, c, d, bad);
+  const Row<R> top{a[0], c[0], d[0]}, bot{a[kTM - 1], c[kTM - 1], d[kTM - 1]};
+  R y[3], z[3];
+  reduced_solve3<R>(top, bot, lane == 0 ? -top.A : R(0), lane == 31 ? -bot.C : R(0), lane, y, z,
+                    bad);
+  R yy = y[0], zz = z[0];
+  if (K > 1) {
+    // the tile's first unknown f = y(lane 0) and last l = z(lane 31), each
+    // as p + alpha x_prev + beta x_next
+    const R pf = shfl_idx(y[0], 0, 32), af = shfl_idx(y[1], 0, 32), bf = shfl_idx(y[2], 0, 32);
+    const R pl = shfl_idx(z[0], 31, 32), al = shfl_idx(z[1], 31, 32), bl = shfl_idx(z[2], 31, 32);
+    bool last = false;
+    if (lane == 0) {
+      // second-level rows:  top  A l_{j-1} + f + C l = D   (x_next eliminated)
+      //                     bot  A f + l + C f_{j+1} = D   (x_prev eliminated)
+      R tA, tC, tDv, bA, bC, bDv;
+      // bl == 0 (no coupling to x_next: then bf == 0 too) and af == 0 (none
+      // to x_prev: al == 0) reduce to the end-of-system forms
+      if (j == K - 1 || bl == R(0)) {
+        tA = -af;
+        tC = R(0);
+        tDv = pf;
+      } else {
+        const R q = bf / bl;
+        tA = -af + q * al;
+        tC = -q;
+        tDv = pf - q * pl;
       }
+      if (j == 0 || af == R(0)) {
+        bA = R(0);
+        bC = -bl;
+        bDv = pl;
+      } else {
+        const R q = al / af;
+        bA = -q;
+        bC = q * bf - bl;
+        bDv = pl - q * pf;
+      }
+      R *tr = p.tile_rows + 6 * (ts + j);
+      tr[0] = tA;
+      tr[1] = tC;
+      tr[2] = tDv;
+      tr[3] = bA;
+      tr[4] = bC;
+      tr[5] = bDv;
+      __threadfence();
+      last = atomicAdd(&p.sys_done[s], 1u) == (unsigned)(K - 1);
     }
-    chunk_forward<R, kBlockM>(a, b, c, d, bad);
-    chunk_backward<R, kBlockM>(a, c, d, bad);
-    const int q = g * kBlockThreads + t;
-    sm_red[0 * Q + q] = a[0];
-    sm_red[1 * Q + q] = c[0];
-    sm_red[2 * Q + q] = d[0];
-    sm_red[3 * Q + q] = a[kBlockM - 1];
-    sm_red[4 * Q + q] = c[kBlockM - 1];
-    sm_red[5 * Q + q] = d[kBlockM - 1];
-  }
-  __syncthreads();
-  // the reduced system (2Q rows): thread t owns chunks [t*NS, (t+1)*NS)
-  {
-    constexpr int K = 2 * NS;
-    R ra[K], rb[K], rc[K], rd[K];
-#pragma unroll
-    for (int j = 0; j < NS; ++j) {
-      const int q = t * NS + j;
-      ra[2 * j] = sm_red[0 * Q + q];
-      rc[2 * j] = sm_red[1 * Q + q];
-      rd[2 * j] = sm_red[2 * Q + q];
-      ra[2 * j + 1] = sm_red[3 * Q + q];
-      rc[2 * j + 1] = sm_red[4 * Q + q];
-      rd[2 * j + 1] = sm_red[5 * Q + q];
-      rb[2 * j] = R(1);
-      rb[2 * j + 1] = R(1);
+    last = __shfl_sync(FULL_MASK, last, 0);
+    if (last) {
+      // every tile's rows are visible (each was fenced before its count)
+      __threadfence();
+      Row<R> t2{R(0), R(0), R(0)}, b2{R(0), R(0), R(0)};
+      if (lane < K) {
+        const R *tr = p.tile_rows + 6 * (ts + lane);  // read from L2, not a stale L1 line
+        t2 = Row<R>{__ldcg(tr + 0), __ldcg(tr + 1), __ldcg(tr + 2)};
+        b2 = Row<R>{__ldcg(tr + 3), __ldcg(tr + 4), __ldcg(tr + 5)};
+      }
+      R f, l;
+      reduced_solve<R>(t2, b2, lane, 32, f, l, bad);
+      if (lane < K) {
+        p.tile_fl[2 * (ts + lane)] = f;
+        p.tile_fl[2 * (ts + lane) + 1] = l;
+      }
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) atomicExch(&p.sys_ready[s], 1u);
+    } else {
+      unsigned ok = 1;
+      if (lane == 0) {
+        // bounded: kWaitLimit polls, and none at all once any wait of this
+        // launch has given up (error != 0)
+        const volatile unsigned *rf = p.sys_ready + s;
+        const volatile unsigned *err = p.error;
+        unsigned it = 0;
+        while (*rf == 0u && *err == 0u && it < kWaitLimit) {
+          __nanosleep(128);
+          ++it;
+        }
+        ok = *rf != 0u;
+        if (!ok) atomicExch(p.error, 2u);
+      }
+      ok = __shfl_sync(FULL_MASK, ok, 0);
+      if (!ok) return;  // reported; this tile is left unsolved
+      __threadfence();
     }
-    chunk_forward<R, K>(ra, rb, rc, rd, bad);
-    chunk_backward<R, K>(ra, rc, rd, bad);
-    R y, z;
-    block_reduced_solve<R, 16>(sm_bs, Row<R>{ra[0], rc[0], rd[0]},
-                               Row<R>{ra[K - 1], rc[K - 1], rd[K - 1]}, 0, t, kBlockThreads, 1, y,
-                               z, bad);
-    chunk_substitute<R, K>(ra, rc, rd, y, z);
-    // the chunks' first and last unknowns; each q is this thread's alone
-#pragma unroll
-    for (int j = 0; j < NS; ++j) {
-      const int q = t * NS + j;
-      sm_red[0 * Q + q] = rd[2 * j];
-      sm_red[1 * Q + q] = rd[2 * j + 1];
-    }
+    const R xp = j > 0 ? __ldcg(p.tile_fl + 2 * (ts + j - 1) + 1) : R(0);
+    const R xn = j < K - 1 ? __ldcg(p.tile_fl + 2 * (ts + j + 1)) : R(0);
+    yy = y[0] + y[1] * xp + y[2] * xn;
+    zz = z[0] + z[1] * xp + z[2] * xn;
   }
-  __syncthreads();
-  // pass B: eliminate every segment again and substitute
-  for (int g = 0; g < NS; ++g) {
-    if ((long long)g * kSegRows >= n) break;  // uniform across the CTA
-    const long long row0 = (long long)g * kSegRows + t * kBlockM;
-    R a[kBlockM], b[kBlockM], c[kBlockM], d[kBlockM];
-    stage_segment<R>(p, base, n, (long long)g * kSegRows, stg);
-    staged_rows<R>(stg, n, (long long)g * kSegRows, a, b, c, d);
-    __syncthreads();
-    chunk_forward<R, kBlockM>(a, b, c, d, bad);
-    chunk_backward<R, kBlockM>(a, c, d, bad);
-    const int q = g * kBlockThreads + t;
-    chunk_substitute<R, kBlockM>(a, c, d, sm_red[0 * Q + q], sm_red[1 * Q + q]);
-    ragged_store<R, kBlockM>(p, base, n, row0, d);
-  }
-  __syncthreads();
+  chunk_substitute<R, kTM>(a, c, d, yy, zz);
+  // x out through the warp's d rows, then coalesced element stores
+  sts_row<R, kTM>(buf + 3 * L::BUF + lane * L::ROW, d);
+  __syncwarp();
+#pragma unroll 4
+  for (int e = lane; e < nt; e += 32) p.d[base0 + r0 + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
+  __syncwarp();  // the buffer is free for the next item
 }
 
 template <typename R>
-__device__ __forceinline__ void block_item_one(const RaggedArgs<R> &p, long long base, long long n,
-                                               R *sm_bs, R *stg, bool &bad) {
-  const int t = threadIdx.x;
-  R a[kBlockM], b[kBlockM], c[kBlockM], d[kBlockM];
-  stage_segment<R>(p, base, n, 0, stg);
-  staged_rows<R>(stg, n, 0, a, b, c, d);
-  chunk_forward<R, kBlockM>(a, b, c, d, bad);
-  chunk_backward<R, kBlockM>(a, c, d, bad);
-  R y, z;
-  block_reduced_solve<R, 16>(sm_bs, Row<R>{a[0], c[0], d[0]},
-                             Row<R>{a[kBlockM - 1], c[kBlockM - 1], d[kBlockM - 1]}, 0, t,
-                             kBlockThreads, 1, y, z, bad);
-  chunk_substitute<R, kBlockM>(a, c, d, y, z);
-  ragged_store<R, kBlockM>(p, base, n, (long long)t * kBlockM, d);
-  __syncthreads();
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kBlockThreads, 1) ragged_kernel(const RaggedArgs<R> p) {
+__global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs<R> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *sm_red = reinterpret_cast<R *>(smem_raw);
-  R *sm_bs = sm_red + 6 * kBlockThreads * kMaxSeg;
-  R *stg = sm_bs + 6 * kBlockThreads * 2;
-  __shared__ long long item;
+  const int lane = threadIdx.x & 31;
+  R *buf = reinterpret_cast<R *>(smem_raw) + (threadIdx.x >> 5) * TileBuf<R>::ELEMS;
+  if (*reinterpret_cast<volatile unsigned *>(p.error) == 3u) return;  // tile table refused
+  long long ntiles = 0, nwarp = 0;
+  for (int c = 0; c < kClasses; ++c) {
+    if (p.mtab[c] == 0)
+      ntiles += (long long)p.tiles[c];
+    else
+      nwarp += p.hist[c];
+  }
   bool bad = false;
-  long long nblock = 0;
-  for (int c = 0; c < kClasses; ++c)
-    if ((1LL << c) > p.warp_max) nblock += p.hist[c];
-  // phase 1: long systems, one per CTA, longest first
   for (;;) {
-    if (threadIdx.x == 0) item = (long long)atomicAdd(&p.counters[0], 1ULL);
-    __syncthreads();
-    const long long it = item;
-    __syncthreads();
-    if (it >= nblock) break;
-    const int s = p.order[it];
-    const long long base = p.off[s];
-    const long long n = p.off[s + 1] - base;
-    if (n > (long long)kSegRows * kMaxSeg) {
-      if (threadIdx.x == 0) *p.error = 1u;
+    long long it = 0;
+    if (lane == 0) it = (long long)atomicAdd(p.counter, 1ULL);
+    it = __shfl_sync(FULL_MASK, it, 0);
+    if (it < ntiles) {
+      const int s = p.tile_sys[it];
+      const long long n = p.off[s + 1] - p.off[s];
+      if (n > (long long)kTileRows * kMaxTiles) {
+        if (lane == 0 && it == p.tstart[s]) atomicExch(p.error, 1u);
+        continue;
+      }
+      tile_item<R>(p, it, buf, lane, bad);
       continue;
     }
-    if (n <= kSegRows)
-      block_item_one<R>(p, base, n, sm_bs, stg, bad);
-    else if (n <= 2LL * kSegRows)
-      block_item_ns<R, 2>(p, base, n, sm_red, sm_bs, stg, bad);
-    else
-      block_item_ns<R, 4>(p, base, n, sm_red, sm_bs, stg, bad);
-  }
-  // phase 2: one system per warp, each warp on its own
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    long long w = 0;
-    if (lane == 0) w = (long long)atomicAdd(&p.counters[1], 1ULL);
-    w = __shfl_sync(FULL_MASK, w, 0);
-    const long long it = nblock + w;
-    if (it >= p.nsys) break;
+    it -= ntiles;
+    if (it >= nwarp) break;
     const int s = p.order[it];
     const long long base = p.off[s];
     const long long n = p.off[s + 1] - base;
-    const int m = p.mtab[length_class(n > 0 ? n : 1)];
-    switch (m) {
+    switch (p.mtab[length_class(n > 0 ? n : 1)]) {
       case 1: warp_item<R, 1>(p, base, n, lane, bad); break;
       case 2: warp_item<R, 2>(p, base, n, lane, bad); break;
       case 4: warp_item<R, 4>(p, base, n, lane, bad); break;
-      case 8: warp_item<R, 8>(p, base, n, lane, bad); break;
-      case 16: warp_item<R, 16>(p, base, n, lane, bad); break;
-      default:
-        if constexpr (sizeof(R) == 4) warp_item<R, 32>(p, base, n, lane, bad);
-        break;
+      default: warp_item<R, 8>(p, base, n, lane, bad); break;
     }
   }
   report_bad_pivot(bad, p.flag);
@@ -353,46 +440,80 @@ __global__ void __launch_bounds__(kBlockThreads, 1) ragged_kernel(const RaggedAr
 
 // ---- host side ---------------------------------------------------------------
 
-// Rows per lane by length class for warp items: built-in table, replaced per
-// device and precision by tridRaggedAutotune.
+// Rows per lane by length class: M > 0 for warp items, 0 for tile classes.
+// Built-in table, replaced per device and precision by tridRaggedAutotune.
 static int g_mtab[2][64][kClasses];
 static bool g_tuned[2][64];
+
+// Longest class a warp per system may take (M <= 8); longer systems take tiles.
+template <typename R> static constexpr int ragged_warp_max() { return 256; }
 
 template <typename R>
 static void default_mtab(int *m) {
   for (int c = 0; c < kClasses; ++c) {
     const long long n = 1LL << c;
-    m[c] = n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : n <= 256 ? 8 : n <= 512 ? 16 : 32;
+    m[c] = n <= 32 ? 1 : n <= 64 ? 2 : 0;
   }
-}
-
-template <typename R> static constexpr int ragged_warp_max() { return sizeof(R) == 8 ? 512 : 1024; }
-
-template <typename R>
-static size_t ragged_smem() {
-  return (size_t)6 * kBlockThreads * kMaxSeg * sizeof(R) +
-         (size_t)6 * kBlockThreads * 2 * sizeof(R) + (size_t)4 * kStageArr * sizeof(R);
 }
 
 template <typename R>
 static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t st) {
   for (int c = 0; c < kClasses; ++c) p.mtab[c] = mtab[c];
-  p.warp_max = ragged_warp_max<R>();
-  // scratch: hist, fill, counters, error, order
-  const size_t head = 256;
+  // classes beyond one warp are always tile classes
+  for (int c = 0; c < kClasses; ++c)
+    if ((1LL << c) > ragged_warp_max<R>()) p.mtab[c] = 0;
+  // the tile scratch is sized by the batch's element count: two offsets
+  // are read back (a short synchronisation on `st`)
+  int64_t ends[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(&ends[0], p.off, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&ends[1], p.off + p.nsys, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  const long long elems = ends[1] - ends[0];
+  if (elems < 0) return cudaErrorInvalidValue;
+  const long long max_tiles = elems / kTileRows + p.nsys + 1;
+  // scratch: header | order (int, nsys) | tstart (i64, nsys) | done, ready
+  // (u32, nsys each) | tile_sys (int, max_tiles) | tile_rows (6 R) | tile_fl (2 R)
+  // header: hist u32[24] @0, fill u32[24] @128, tiles u64[24] @256,
+  //         tfill u64[24] @512, counter u64 @768, error u32 @776
+  const size_t head = 1024;
+  auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+  const size_t o_order = head;
+  const size_t o_tstart = o_order + up((size_t)p.nsys * sizeof(int));
+  const size_t o_done = o_tstart + up((size_t)p.nsys * sizeof(long long));
+  const size_t o_ready = o_done + up((size_t)p.nsys * sizeof(unsigned));
+  const size_t o_tsys = o_ready + up((size_t)p.nsys * sizeof(unsigned));
+  const size_t o_trows = o_tsys + up((size_t)max_tiles * sizeof(int));
+  const size_t o_tfl = o_trows + up((size_t)max_tiles * 6 * sizeof(R));
+  const size_t total = o_tfl + up((size_t)max_tiles * 2 * sizeof(R));
   char *scratch = nullptr;
-  cudaError_t e = cudaMallocAsync((void **)&scratch, head + (size_t)p.nsys * sizeof(int), st);
+  e = scratch_alloc((void **)&scratch, total, st);
   if (e != cudaSuccess) return e;
   unsigned *hist = reinterpret_cast<unsigned *>(scratch);
-  unsigned *fill = hist + kClasses;
-  // hist [0, 96), fill [96, 192), counters [192, 208), error [208, 212)
-  unsigned long long *counters = reinterpret_cast<unsigned long long *>(scratch + 192);
-  unsigned *error = reinterpret_cast<unsigned *>(scratch + 208);
-  int *order = reinterpret_cast<int *>(scratch + head);
+  unsigned *fill = reinterpret_cast<unsigned *>(scratch + 128);
+  unsigned long long *tiles = reinterpret_cast<unsigned long long *>(scratch + 256);
+  unsigned long long *tfill = reinterpret_cast<unsigned long long *>(scratch + 512);
+  unsigned long long *counter = reinterpret_cast<unsigned long long *>(scratch + 768);
+  unsigned *error = reinterpret_cast<unsigned *>(scratch + 776);
+  int *order = reinterpret_cast<int *>(scratch + o_order);
+  long long *tstart = reinterpret_cast<long long *>(scratch + o_tstart);
+  unsigned *done = reinterpret_cast<unsigned *>(scratch + o_done);
+  unsigned *ready = reinterpret_cast<unsigned *>(scratch + o_ready);
+  int *tile_sys = reinterpret_cast<int *>(scratch + o_tsys);
   e = cudaMemsetAsync(scratch, 0, head, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(scratch + o_done, 0, o_tsys - o_done, st);
   p.hist = hist;
-  p.counters = counters;
+  p.tiles = tiles;
   p.order = order;
+  p.tstart = tstart;
+  p.tile_sys = tile_sys;
+  p.tile_rows = reinterpret_cast<R *>(scratch + o_trows);
+  p.tile_fl = reinterpret_cast<R *>(scratch + o_tfl);
+  p.sys_done = done;
+  p.sys_ready = ready;
+  p.max_tiles = max_tiles;
+  p.counter = counter;
   p.error = error;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -400,30 +521,32 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   if (e == cudaSuccess) {
     const long long g = (p.nsys + 255) / 256;
     const unsigned grid = (unsigned)(g < 4LL * sms ? (g > 0 ? g : 1) : 4LL * sms);
-    ragged_hist_kernel<R><<<grid, 256, 0, st>>>(p, hist);
-    ragged_order_kernel<R><<<grid, 256, 0, st>>>(p, hist, fill, order);
+    ragged_hist_kernel<R><<<grid, 256, 0, st>>>(p, hist, tiles);
+    ragged_order_kernel<R><<<grid, 256, 0, st>>>(p, hist, tiles, fill, tfill, order, tile_sys, tstart);
     g_launches.fetch_add(2, std::memory_order_relaxed);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
-    const size_t smem = ragged_smem<R>();
+    const size_t smem = (size_t)(kRaggedThreads / 32) * TileBuf<R>::ELEMS * sizeof(R);
     cudaFuncSetAttribute(ragged_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ragged_kernel<R>, kBlockThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ragged_kernel<R>, kRaggedThreads, smem);
     if (per_sm < 1) per_sm = 1;
-    ragged_kernel<R><<<(unsigned)(sms * per_sm), kBlockThreads, smem, st>>>(p);
+    // every CTA resident at once (the waits rely on running warps only)
+    ragged_kernel<R><<<(unsigned)(sms * per_sm), kRaggedThreads, smem, st>>>(p);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
   }
-  // a system longer than the block-item limit sets `error`; it can only be
-  // read back when the call blocks
+  // errors recorded by the kernel can only be read back when the call blocks
   if (e == cudaSuccess && settings().blocking) {
     unsigned h = 0;
     e = cudaMemcpyAsync(&h, error, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess && h) e = cudaErrorNotSupported;
+    if (e == cudaSuccess && h == 1u) e = cudaErrorNotSupported;
+    if (e == cudaSuccess && h == 3u) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess && h >= 2u) e = cudaErrorLaunchFailure;
   }
-  cudaError_t ef = cudaFreeAsync(scratch, st);
+  cudaError_t ef = scratch_free(scratch, st);
   return e != cudaSuccess ? e : ef;
 }
 
@@ -459,6 +582,7 @@ static tridStatus_t ragged(const R *a, const R *b, const R *c, R *d, const int64
   if (cfg.blocking) pivot_flag_take();
   cudaError_t e = launch_ragged<R>(p, mt, cfg.stream);
   if (e == cudaErrorNotSupported) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
+  if (e == cudaErrorInvalidValue) return TRID_STATUS_INVALID_VALUE;
   if (e != cudaSuccess) return status_of(e);
   if (cfg.blocking) {
     e = cudaStreamSynchronize(cfg.stream);
@@ -486,8 +610,9 @@ __global__ void ragged_fill_kernel(R *a, R *b, R *c, R *d, int64_t *off, long lo
 }
 
 // For every length class a warp item can take, times each rows-per-lane
-// choice that holds the class (32*M >= 2^class) on a uniform batch of that
-// class and keeps the fastest. Block items are not tuned (one shape).
+// choice that holds the class (32*M >= 2^class) and the staged 512-row tile
+// (table entry 0) on a uniform batch of that class, and keeps the fastest.
+// Longer classes always take tiles.
 template <typename R>
 static tridStatus_t autotune(int dev) {
   int mt[kClasses];
@@ -516,8 +641,8 @@ static tridStatus_t autotune(int dev) {
                                                 nsys * len, len, nsys);
     float best = 1e30f;
     int best_m = mt[cls];
-    for (int m = 1; m <= (sizeof(R) == 4 ? 32 : 16); m *= 2) {
-      if (32LL * m < len) continue;
+    for (int m = 0; m <= 8; m = m ? 2 * m : 1) {
+      if (m > 0 && 32LL * m < len) continue;
       int trial[kClasses];
       memcpy(trial, mt, sizeof(trial));
       trial[cls] = m;
