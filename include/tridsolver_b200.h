@@ -131,6 +131,35 @@ EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const TridParams *ctx, const 
                                                    float *bbar, float *cbar, int ndim,
                                                    int solvedim, const int *dims, const int *pads);
 
+/* ---- generic strided batch -------------------------------------------------
+ * The surface of the reference's solveBatchedTrid
+ * (scalar/src/cuda/trid_thomaspcr.hpp:794-832, a C++ template there): numTrids
+ * systems of `length` rows, rows stride1 elements apart; system k starts at
+ * k*stride2 when stride1 == 1, else at (k / subBatchSize)*subBatchStride +
+ * (k % subBatchSize)*stride2 (e.g. a y solve of an X*Y*Z cube: stride1 = X,
+ * stride2 = 1, subBatchSize = X, subBatchStride = X*Y). d is read and x
+ * written (Inc: x += solution); a[0] and c[length-1] are treated as zero.
+ * Unlike the reference, any combination of strides is accepted (it requires
+ * stride1 == 1 or stride2 == 1), a last partial sub-batch is allowed, and a
+ * status is returned instead of 0/1. */
+EXTERN_C tridStatus_t tridDsolveBatchedTrid(const TridParams *ctx, int numTrids, int length,
+                                            int stride1, int stride2, int subBatchSize,
+                                            int subBatchStride, const double *a, const double *b,
+                                            const double *c, const double *d, double *x);
+EXTERN_C tridStatus_t tridSsolveBatchedTrid(const TridParams *ctx, int numTrids, int length,
+                                            int stride1, int stride2, int subBatchSize,
+                                            int subBatchStride, const float *a, const float *b,
+                                            const float *c, const float *d, float *x);
+EXTERN_C tridStatus_t tridDsolveBatchedTridInc(const TridParams *ctx, int numTrids, int length,
+                                               int stride1, int stride2, int subBatchSize,
+                                               int subBatchStride, const double *a,
+                                               const double *b, const double *c, const double *d,
+                                               double *x);
+EXTERN_C tridStatus_t tridSsolveBatchedTridInc(const TridParams *ctx, int numTrids, int length,
+                                               int stride1, int stride2, int subBatchSize,
+                                               int subBatchStride, const float *a, const float *b,
+                                               const float *c, const float *d, float *x);
+
 /* ---- FP32 storage, FP64 accuracy -----------------------------------------
  * No counterpart in the reference. Solves T x = d where a, b, c are stored in
  * FP32 (the system is exactly those values, promoted to FP64) and d is FP64;

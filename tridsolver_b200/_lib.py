@@ -24,6 +24,10 @@ SYMBOLS = {
     "tridDmtsvStridedBatchInc": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _IP, _IP]),
     "tridSmtsvStridedBatchInc": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _IP, _IP]),
     # extensions, include/tridsolver_b200.h
+    "tridDsolveBatchedTrid": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "tridSsolveBatchedTrid": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "tridDsolveBatchedTridInc": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "tridSsolveBatchedTridInc": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
     "tridSetStream": (_I, [_P]),
     "tridGetStream": (_P, []),
     "tridSetBlocking": (_I, [_I]),

@@ -101,6 +101,18 @@ def tridSmtsvStridedBatchInc(ctx, a, b, c, d, u, ndim, solvedim, dims, pads):
                                                 _ints(pads))
 
 
+def solve_batched_trid(num_trids, length, stride1, stride2, sub_batch_size, sub_batch_stride, a, b,
+                       c, d, x, inc=False, ctx=None):
+    """The reference's solveBatchedTrid surface (include/tridsolver_b200.h):
+    FP64 or FP32 by the tensors' dtype; x receives the solution (x += it
+    when inc). Returns the status."""
+    f64 = getattr(a, "dtype", None) is None or str(a.dtype).endswith("float64")
+    name = ("tridDsolveBatchedTrid" if f64 else "tridSsolveBatchedTrid") + ("Inc" if inc else "")
+    return getattr(_lib.load(), name)(_ctx(ctx), int(num_trids), int(length), int(stride1),
+                                      int(stride2), int(sub_batch_size), int(sub_batch_stride),
+                                      _addr(a), _addr(b), _addr(c), _addr(d), _addr(x))
+
+
 def tridDmtsvStridedBatchMixed(ctx, a, b, c, d, ndim, solvedim, dims, pads, max_iters=10,
                                tol=1e-12):
     """FP32-stored a, b, c; FP64 d (x overwrites it); FP32 solves refined in

@@ -167,9 +167,116 @@ static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b,
   return TRID_STATUS_SUCCESS;
 }
 
+// The generic surface of the reference's solveBatchedTrid
+// (scalar/src/cuda/trid_thomaspcr.hpp:794-832): system k starts at
+//   stride1 == 1:  k * stride2
+//   otherwise:     (k / subBatchSize) * subBatchStride + (k % subBatchSize) * stride2
+// and its rows are stride1 apart; d is read, x written (x += solution for
+// Inc). That is BatchArgs with n0 = subBatchSize, st0 = stride2,
+// st1 = subBatchStride; a last, partial sub-batch is a second launch.
+template <typename R, bool INC>
+static tridStatus_t solve_batched(const TridParams *ctx, int numTrids, int length, int stride1,
+                                  int stride2, int subBatchSize, int subBatchStride, const R *a,
+                                  const R *b, const R *c, const R *d, R *x) {
+  (void)ctx;
+  if (numTrids < 0 || length < 0 || stride1 < 1 || stride2 < 0 || subBatchStride < 0)
+    return TRID_STATUS_INVALID_VALUE;
+  if (numTrids == 0 || length == 0) return TRID_STATUS_SUCCESS;
+  if (!a || !b || !c || !d || !x || (stride1 != 1 && subBatchSize < 1)) return TRID_STATUS_INVALID_VALUE;
+  tridStatus_t st = check_device();
+  if (st != TRID_STATUS_SUCCESS) return st;
+  const Settings &cfg = settings();
+  BatchArgs<R> p{};
+  p.a = a;
+  p.b = b;
+  p.c = c;
+  p.d_in = d;
+  p.d_out = INC ? nullptr : x;
+  p.u = INC ? x : nullptr;
+  p.N = length;
+  p.stride = stride1;
+  p.flag = pivot_flag_device();
+  if (cfg.blocking) pivot_flag_take();
+  auto run = [&](const BatchArgs<R> &q) -> cudaError_t {
+    const Plan plan = choose_plan<R>(q, vec_aligned<R>(q));
+    return launch_batch<R, INC>(q, plan, cfg.stream);
+  };
+  cudaError_t e = cudaSuccess;
+  if (stride1 == 1) {
+    p.n0 = numTrids;
+    p.nsys = numTrids;
+    p.st0 = stride2;
+    p.st1 = 0;
+    e = run(p);
+  } else {
+    const long long full = numTrids / subBatchSize, rem = numTrids % subBatchSize;
+    p.n0 = subBatchSize;
+    p.st0 = stride2;
+    p.st1 = subBatchStride;
+    if (full > 0) {
+      p.nsys = full * subBatchSize;
+      e = run(p);
+    }
+    if (e == cudaSuccess && rem > 0) {
+      const long long o = full * (long long)subBatchStride;
+      BatchArgs<R> q = p;
+      q.a = a + o;
+      q.b = b + o;
+      q.c = c + o;
+      q.d_in = d + o;
+      q.d_out = INC ? nullptr : x + o;
+      q.u = INC ? x + o : nullptr;
+      q.n0 = rem;
+      q.nsys = rem;
+      q.st1 = 0;
+      e = run(q);
+    }
+  }
+  if (e != cudaSuccess) return status_of(e);
+  if (cfg.blocking) {
+    e = cudaStreamSynchronize(cfg.stream);
+    if (e != cudaSuccess) return status_of(e);
+    if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
 }  // namespace trid
 
 using namespace trid;
+
+EXTERN_C tridStatus_t tridDsolveBatchedTrid(const TridParams *ctx, int numTrids, int length,
+                                            int stride1, int stride2, int subBatchSize,
+                                            int subBatchStride, const double *a, const double *b,
+                                            const double *c, const double *d, double *x) {
+  return solve_batched<double, false>(ctx, numTrids, length, stride1, stride2, subBatchSize,
+                                      subBatchStride, a, b, c, d, x);
+}
+
+EXTERN_C tridStatus_t tridSsolveBatchedTrid(const TridParams *ctx, int numTrids, int length,
+                                            int stride1, int stride2, int subBatchSize,
+                                            int subBatchStride, const float *a, const float *b,
+                                            const float *c, const float *d, float *x) {
+  return solve_batched<float, false>(ctx, numTrids, length, stride1, stride2, subBatchSize,
+                                     subBatchStride, a, b, c, d, x);
+}
+
+EXTERN_C tridStatus_t tridDsolveBatchedTridInc(const TridParams *ctx, int numTrids, int length,
+                                               int stride1, int stride2, int subBatchSize,
+                                               int subBatchStride, const double *a,
+                                               const double *b, const double *c, const double *d,
+                                               double *x) {
+  return solve_batched<double, true>(ctx, numTrids, length, stride1, stride2, subBatchSize,
+                                     subBatchStride, a, b, c, d, x);
+}
+
+EXTERN_C tridStatus_t tridSsolveBatchedTridInc(const TridParams *ctx, int numTrids, int length,
+                                               int stride1, int stride2, int subBatchSize,
+                                               int subBatchStride, const float *a, const float *b,
+                                               const float *c, const float *d, float *x) {
+  return solve_batched<float, true>(ctx, numTrids, length, stride1, stride2, subBatchSize,
+                                    subBatchStride, a, b, c, d, x);
+}
 
 EXTERN_C tridStatus_t tridDmtsvStridedBatch(const TridParams *ctx, const double *a, const double *b,
                                             const double *c, double *d, int ndim, int solvedim,

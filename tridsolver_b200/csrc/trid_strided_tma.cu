@@ -28,7 +28,7 @@
 namespace trid {
 
 struct TmaMaps {
-  CUtensorMap m[5];  // a, b, c, d, u
+  CUtensorMap m[5];  // a, b, c, d (loads); [4]: the output, u for Inc, else d_out
 };
 
 constexpr unsigned kTmaWaitLimit = 1u << 22;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256, 1)
       for (int box = 0; box < nbox; ++box) {
         int c0, c1, c2;
         coords(g, box, c0, c1, c2);
-        tma_store_3d(&maps.m[OUT], c0, c1, c2, tl + OUT * tile + box * rows_box * W);
+        tma_store_3d(&maps.m[4], c0, c1, c2, tl + OUT * tile + box * rows_box * W);
       }
       tma_store_commit();
       if (stages == 1) {
@@ -186,7 +186,7 @@ bool tma_geometry(const BatchArgs<R> &p, bool inc, int W, int &rows_box, int &nb
                   size_t &smem, int T) {
   if (p.stride == 1 || p.N > 1024 || p.N < 1 || W < 1) return false;
   auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
-  if (!al(p.a) || !al(p.b) || !al(p.c) || !al(p.d_in) || (inc && !al(p.u))) return false;
+  if (!al(p.a) || !al(p.b) || !al(p.c) || !al(p.d_in) || !al(inc ? p.u : p.d_out)) return false;
   const long long es = sizeof(R);
   if ((p.stride * es) % 16 || (p.st1 * es) % 16 || p.st0 != 1) return false;
   if ((W * es) % 16) return false;
@@ -247,10 +247,10 @@ cudaError_t launch_strided_tma(const BatchArgs<R> &p, const Plan &plan, cudaStre
   const cuuint32_t estr[3] = {1, 1, 1};
   TmaMaps maps;
   memset(&maps, 0, sizeof(maps));
-  const void *ptrs[5] = {p.a, p.b, p.c, p.d_in, INC ? p.u : p.d_in};
+  const void *ptrs[5] = {p.a, p.b, p.c, p.d_in, INC ? p.u : p.d_out};
   const CUtensorMapDataType dt =
       sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  for (int k = 0; k < (INC ? 5 : 4); ++k) {
+  for (int k = 0; k < 5; ++k) {
     CUresult r = enc(&maps.m[k], dt, 3, const_cast<void *>(ptrs[k]), gdim, gstr, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
