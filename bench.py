@@ -47,6 +47,11 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--only-config", default=None,
+                    choices=["sweep", "adi", "precision", "ragged", "adjoint"],
+                    help="run just one of the other configurations and print its JSON (profiling)")
+    ap.add_argument("--ragged-systems", type=int, default=200000,
+                    help="systems in the ragged configuration (200000 = the benchmark)")
     ap.add_argument("--grid", default=None,
                     help="X,Y,Z grid instead of n^3 (smaller cases for profiling; x fastest)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -432,16 +437,17 @@ def config_adi(dev, hbm, n=(256, 256, 256), steps=100, dtype="f64", alpha=1.0):
             "finite": bool(torch.isfinite(sim.u).all().item())}
 
 
-def config_precision(dev, n=512):
+def config_precision(dev, n=512, dims=None):
     """FP32 storage + FP32 solve with on-chip FP64 refinement vs the plain FP64
     solve, along x and z, margins log-uniform [10^lo, 1]."""
     import torch
     import tridsolver_b200 as tb
     stream = torch.cuda.current_stream()
-    dims = [n] * 3
+    dims = list(dims) if dims else [n] * 3
+    shape = tuple(reversed(dims))
     out = []
     for lo in (-3, -2, -1, 0):
-        a, b, c, d = _system((n, n, n), torch.float64, dev, 7 - lo, margin_lo=lo if lo < 0 else None)
+        a, b, c, d = _system(shape, torch.float64, dev, 7 - lo, margin_lo=lo if lo < 0 else None)
         a32, b32, c32 = a.float(), b.float(), c.float()
         del a, b, c
         a64, b64, c64 = a32.double(), b32.double(), c32.double()
@@ -594,6 +600,21 @@ def run_configs(dev, hbm):
 
 def main():
     args = parse_args()
+    if args.only_config:
+        import torch
+        import tridsolver_b200 as tb
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        tb.set_stream(torch.cuda.current_stream())
+        tb.set_blocking(False)
+        hbm = peaks()[0]
+        grid = [int(v) for v in args.grid.split(",")] if args.grid else None
+        fn = {"sweep": lambda: config_sweep(dev, hbm), "adi": lambda: config_adi(dev, hbm),
+              "precision": lambda: config_precision(dev, args.n, grid),
+              "ragged": lambda: config_ragged(dev, hbm, args.ragged_systems),
+              "adjoint": lambda: config_adjoint(dev)}[args.only_config]
+        print(json.dumps({"config": args.only_config, "result": fn()}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
