@@ -68,6 +68,20 @@ template <typename R> struct RaggedArgs {
   long long max_tiles;              // entries of tile_sys / tile_rows / tile_fl
 };
 
+// Release/acquire operations at device scope: a tile's second-level rows are
+// published by the count that follows them, and read after the count
+// (acquire) by the warp that completes the system.
+__device__ __forceinline__ unsigned atomic_add_acq_rel(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ int length_class(long long n) {
   int c = 0;
   while (c < kClasses - 1 && (1LL << c) < n) ++c;
@@ -340,13 +354,13 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
       tr[3] = bA;
       tr[4] = bC;
       tr[5] = bDv;
-      __threadfence();
-      last = atomicAdd(&p.sys_done[s], 1u) == (unsigned)(K - 1);
+      // release: the rows before the count; acquire: the other tiles' rows
+      // for the warp that completes the count
+      last = atomic_add_acq_rel(&p.sys_done[s], 1u) == (unsigned)(K - 1);
     }
     last = __shfl_sync(FULL_MASK, last, 0);
     if (last) {
-      // every tile's rows are visible (each was fenced before its count)
-      __threadfence();
+      __syncwarp();
       Row<R> t2{R(0), R(0), R(0)}, b2{R(0), R(0), R(0)};
       if (lane < K) {
         const R *tr = p.tile_rows + 6 * (ts + lane);  // read from L2, not a stale L1 line
@@ -367,19 +381,20 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
       if (lane == 0) {
         // bounded: kWaitLimit polls, and none at all once any wait of this
         // launch has given up (error != 0)
-        const volatile unsigned *rf = p.sys_ready + s;
         const volatile unsigned *err = p.error;
         unsigned it = 0;
-        while (*rf == 0u && *err == 0u && it < kWaitLimit) {
+        unsigned r = load_acquire(p.sys_ready + s);
+        while (r == 0u && *err == 0u && it < kWaitLimit) {
           __nanosleep(128);
           ++it;
+          r = load_acquire(p.sys_ready + s);
         }
-        ok = *rf != 0u;
+        ok = r != 0u;
         if (!ok) atomicExch(p.error, 2u);
       }
       ok = __shfl_sync(FULL_MASK, ok, 0);
       if (!ok) return;  // reported; this tile is left unsolved
-      __threadfence();
+      __syncwarp();
     }
     const R xp = j > 0 ? __ldcg(p.tile_fl + 2 * (ts + j - 1) + 1) : R(0);
     const R xn = j < K - 1 ? __ldcg(p.tile_fl + 2 * (ts + j + 1)) : R(0);
