@@ -53,8 +53,8 @@ template <typename R> struct RaggedArgs {
   const int *order;                 // warp-item systems, longest class first
   const unsigned *hist;             // systems per class
   const unsigned long long *tiles;  // tiles per class (tile classes)
-  const int *tile_sys;              // system of each tile item
-  const long long *tstart;          // first tile item of each (tile-class) system
+  const int4 *tile_meta;            // per tile item: system, tile index j, tiles K, rows n
+  const long long *tile_base;       // per tile item: the system's first element
   R *tile_rows;                     // 6 per tile: top A, C, D; bottom A, C, D
   R *tile_fl;                       // 2 per tile: first and last unknown
   unsigned *sys_done;               // tiles of the system past the reduction
@@ -65,7 +65,8 @@ template <typename R> struct RaggedArgs {
   unsigned *flag;
   unsigned *error;                  // 1: a system longer than 16384 rows; 2: a wait gave up;
                                     // 3: the tile table was too small
-  long long max_tiles;              // entries of tile_sys / tile_rows / tile_fl
+  long long max_tiles;              // entries of tile_meta / tile_base / tile_rows / tile_fl
+  bool vec16;                       // a, b, c, d all 16-byte aligned
 };
 
 // Release/acquire operations at device scope: a tile's second-level rows are
@@ -102,8 +103,8 @@ __global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist, unsigned lon
 template <typename R>
 __global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist,
                                     const unsigned long long *tiles, unsigned *fill,
-                                    unsigned long long *tfill, int *order, int *tile_sys,
-                                    long long *tstart) {
+                                    unsigned long long *tfill, int *order, int4 *tile_meta,
+                                    long long *tile_base) {
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < p.nsys;
        s += (long long)gridDim.x * blockDim.x) {
     const long long n = p.off[s + 1] - p.off[s];
@@ -114,12 +115,16 @@ __global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist,
         if (p.mtab[q] == 0) t0 += tiles[q];
       const long long K = (n + kTileRows - 1) / kTileRows;
       const long long ts = (long long)(t0 + atomicAdd(&tfill[c], (unsigned long long)K));
-      tstart[s] = ts;
       if (ts + K > p.max_tiles) {  // offsets not ascending: refuse rather than overrun
         atomicExch(p.error, 3u);
         continue;
       }
-      for (long long j = 0; j < K; ++j) tile_sys[ts + j] = (int)s;
+      const long long base = p.off[s];
+      for (long long j = 0; j < K; ++j) {
+        tile_meta[ts + j] = make_int4((int)s, (int)j, (int)(K < 0x7fffffff ? K : 0x7fffffff),
+                                      (int)(n < 0x7fffffff ? n : 0x7fffffff));
+        tile_base[ts + j] = base;
+      }
     } else {
       unsigned start = 0;
       for (int q = kClasses - 1; q > c; --q)
@@ -259,14 +264,31 @@ template <typename R> struct TileBuf {
 };
 
 // Copies rows [0, nt) of the tile starting at element `base` into the warp's
-// buffer (element-sized cp.async: 32 consecutive elements per instruction,
-// any alignment); rows nt..511 become identity rows.
+// buffer and makes rows nt..511 identity rows. 16-byte cp.async units where
+// the tile's start is 16-byte aligned (each unit lies inside one lane's
+// chunk row, whose padded start is 16-byte aligned), element-sized copies
+// otherwise (32 consecutive elements per instruction) and for the tail.
 template <typename R>
 __device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long base, int nt, R *buf,
                                            int lane) {
   using L = SmemLayout<R, kTM>;
+  constexpr int V = 16 / (int)sizeof(R);
+  int e0 = 0;
+  if (p.vec16 && base % V == 0) {
+    const int nfull = nt / V;
 #pragma unroll 4
-  for (int e = lane; e < kTileRows; e += 32) {
+    for (int u = lane; u < nfull; u += 32) {
+      const int e = u * V;
+      const int o = TileBuf<R>::slot(e);
+      cp_async16(buf + 0 * L::BUF + o, p.a + base + e, 16);
+      cp_async16(buf + 1 * L::BUF + o, p.b + base + e, 16);
+      cp_async16(buf + 2 * L::BUF + o, p.c + base + e, 16);
+      cp_async16(buf + 3 * L::BUF + o, p.d + base + e, 16);
+    }
+    e0 = nfull * V;
+  }
+#pragma unroll 4
+  for (int e = e0 + lane; e < kTileRows; e += 32) {
     const int o = TileBuf<R>::slot(e);
     if (e < nt) {
       cp_async_elem<R>(buf + 0 * L::BUF + o, p.a + base + e);
@@ -288,12 +310,13 @@ template <typename R>
 __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item, R *buf, int lane,
                                           bool &bad) {
   using L = SmemLayout<R, kTM>;
-  const int s = p.tile_sys[item];
-  const long long ts = p.tstart[s];
-  const int j = (int)(item - ts);
-  const long long base0 = p.off[s];
-  const long long n = p.off[s + 1] - base0;
-  const int K = (int)((n + kTileRows - 1) / kTileRows);
+  const int4 meta = p.tile_meta[item];
+  const int s = meta.x;
+  const int j = meta.y;
+  const int K = meta.z;
+  const long long n = meta.w;
+  const long long ts = item - j;
+  const long long base0 = p.tile_base[item];
   const long long r0 = (long long)j * kTileRows;
   const int nt = (int)(n - r0 < kTileRows ? n - r0 : kTileRows);
   stage_tile<R>(p, base0 + r0, nt, buf, lane);
@@ -429,10 +452,9 @@ __global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs
     if (lane == 0) it = (long long)atomicAdd(p.counter, 1ULL);
     it = __shfl_sync(FULL_MASK, it, 0);
     if (it < ntiles) {
-      const int s = p.tile_sys[it];
-      const long long n = p.off[s + 1] - p.off[s];
-      if (n > (long long)kTileRows * kMaxTiles) {
-        if (lane == 0 && it == p.tstart[s]) atomicExch(p.error, 1u);
+      const int4 meta = p.tile_meta[it];
+      if (meta.z > kMaxTiles) {  // longer than 16384 rows: reported once per system
+        if (lane == 0 && meta.y == 0) atomicExch(p.error, 1u);
         continue;
       }
       tile_item<R>(p, it, buf, lane, bad);
@@ -488,18 +510,18 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   const long long elems = ends[1] - ends[0];
   if (elems < 0) return cudaErrorInvalidValue;
   const long long max_tiles = elems / kTileRows + p.nsys + 1;
-  // scratch: header | order (int, nsys) | tstart (i64, nsys) | done, ready
-  // (u32, nsys each) | tile_sys (int, max_tiles) | tile_rows (6 R) | tile_fl (2 R)
+  // scratch: header | order (int, nsys) | done, ready (u32, nsys each) |
+  // tile_meta (int4, max_tiles) | tile_base (i64) | tile_rows (6 R) | tile_fl (2 R)
   // header: hist u32[24] @0, fill u32[24] @128, tiles u64[24] @256,
   //         tfill u64[24] @512, counter u64 @768, error u32 @776
   const size_t head = 1024;
   auto up = [](size_t v) { return (v + 255) / 256 * 256; };
   const size_t o_order = head;
-  const size_t o_tstart = o_order + up((size_t)p.nsys * sizeof(int));
-  const size_t o_done = o_tstart + up((size_t)p.nsys * sizeof(long long));
+  const size_t o_done = o_order + up((size_t)p.nsys * sizeof(int));
   const size_t o_ready = o_done + up((size_t)p.nsys * sizeof(unsigned));
-  const size_t o_tsys = o_ready + up((size_t)p.nsys * sizeof(unsigned));
-  const size_t o_trows = o_tsys + up((size_t)max_tiles * sizeof(int));
+  const size_t o_tmeta = o_ready + up((size_t)p.nsys * sizeof(unsigned));
+  const size_t o_tbase = o_tmeta + up((size_t)max_tiles * sizeof(int4));
+  const size_t o_trows = o_tbase + up((size_t)max_tiles * sizeof(long long));
   const size_t o_tfl = o_trows + up((size_t)max_tiles * 6 * sizeof(R));
   const size_t total = o_tfl + up((size_t)max_tiles * 2 * sizeof(R));
   char *scratch = nullptr;
@@ -512,17 +534,21 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   unsigned long long *counter = reinterpret_cast<unsigned long long *>(scratch + 768);
   unsigned *error = reinterpret_cast<unsigned *>(scratch + 776);
   int *order = reinterpret_cast<int *>(scratch + o_order);
-  long long *tstart = reinterpret_cast<long long *>(scratch + o_tstart);
   unsigned *done = reinterpret_cast<unsigned *>(scratch + o_done);
   unsigned *ready = reinterpret_cast<unsigned *>(scratch + o_ready);
-  int *tile_sys = reinterpret_cast<int *>(scratch + o_tsys);
+  int4 *tile_meta = reinterpret_cast<int4 *>(scratch + o_tmeta);
+  long long *tile_base = reinterpret_cast<long long *>(scratch + o_tbase);
   e = cudaMemsetAsync(scratch, 0, head, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(scratch + o_done, 0, o_tsys - o_done, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(scratch + o_done, 0, o_tmeta - o_done, st);
   p.hist = hist;
   p.tiles = tiles;
   p.order = order;
-  p.tstart = tstart;
-  p.tile_sys = tile_sys;
+  p.tile_meta = tile_meta;
+  p.tile_base = tile_base;
+  {
+    auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    p.vec16 = al(p.a) && al(p.b) && al(p.c) && al(p.d);
+  }
   p.tile_rows = reinterpret_cast<R *>(scratch + o_trows);
   p.tile_fl = reinterpret_cast<R *>(scratch + o_tfl);
   p.sys_done = done;
@@ -537,7 +563,8 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
     const long long g = (p.nsys + 255) / 256;
     const unsigned grid = (unsigned)(g < 4LL * sms ? (g > 0 ? g : 1) : 4LL * sms);
     ragged_hist_kernel<R><<<grid, 256, 0, st>>>(p, hist, tiles);
-    ragged_order_kernel<R><<<grid, 256, 0, st>>>(p, hist, tiles, fill, tfill, order, tile_sys, tstart);
+    ragged_order_kernel<R><<<grid, 256, 0, st>>>(p, hist, tiles, fill, tfill, order, tile_meta,
+                                                 tile_base);
     g_launches.fetch_add(2, std::memory_order_relaxed);
     e = cudaGetLastError();
   }
