@@ -27,7 +27,10 @@ def oracle():
 
 
 SHAPES = [([64, 12, 5], 0), ([9, 40, 6], 1), ([7, 5, 33], 2), ([512, 3], 0), ([6, 700], 1),
-          ([1, 1, 1], 2), ([2, 2], 1), ([16, 256, 4], 1)]
+          ([1, 1, 1], 2), ([2, 2], 1), ([16, 256, 4], 1),
+          # the streaming kernel's adjoint form (strided, 64 < N <= 512): every
+          # chunk size, partial groups and chunks, y and z layouts
+          ([32, 100, 3], 1), ([20, 5, 300], 2), ([48, 2, 512], 2), ([16, 129, 2], 1)]
 
 
 @pytest.mark.parametrize("products", [True, False])
@@ -51,8 +54,31 @@ def test_adjoint_against_oracle(dims, solvedim, products, oracle):
             assert normwise(got.cpu().numpy(), ref) <= 1e-12
 
 
-def test_adjoint_fp32(oracle):
-    dims, sd = [20, 30, 4], 1
+@pytest.mark.parametrize("which", [(True, False, False), (False, True, True), (False, False, True)])
+def test_adjoint_some_products(which, oracle):
+    """Only some of abar, bbar, cbar asked for (the others null), on the
+    streaming path: the ones asked for match the oracle, dbar too."""
+    dims, sd = [24, 7, 260], 2
+    a, b, c, d = make_system(dims, sd, np.float64, seed=8)
+    x = d.copy()
+    oracle.strided_batch(a, b, c, x, dims, sd)
+    w = np.random.default_rng(2).standard_normal(d.size)
+    want = oracle.adjoint(a, b, c, x, w, dims, sd)
+    ta, tb_, tc, tx, tw = (torch.from_numpy(v).cuda() for v in (a, b, c, x, w))
+    outs = [torch.full_like(tx, np.nan) if k < 3 and which[k] else None for k in range(3)]
+    dbar = torch.full_like(tx, np.nan)
+    st = tb.tridDmtsvStridedBatchAdjoint(None, ta, tb_, tc, tx, tw, dbar, outs[0], outs[1], outs[2],
+                                         3, sd, dims, dims)
+    torch.cuda.synchronize()
+    assert st == 0
+    assert normwise(dbar.cpu().numpy(), want[3]) <= 1e-12
+    for k in range(3):
+        if which[k]:
+            assert normwise(outs[k].cpu().numpy(), want[k]) <= 1e-12
+
+
+@pytest.mark.parametrize("dims,sd", [([20, 30, 4], 1), ([40, 3, 200], 2)])
+def test_adjoint_fp32(dims, sd, oracle):
     a, b, c, d = make_system(dims, sd, np.float64, seed=3)
     x = d.copy()
     oracle.strided_batch(a, b, c, x, dims, sd)

@@ -8,7 +8,9 @@
 // super-diagonal a_{i+1}, so the transposed solve is the forward partition
 // hybrid fed with a and c shifted by one row; the three products are fused
 // into the same pass, which reads a, b, c, w, x once and writes the four
-// gradients once (9 words per element; 5 when only dbar is wanted).
+// gradients once (9 words per element; 5 when only dbar is wanted). Strided
+// batches of 64 < N <= 512 use the streaming kernel's adjoint form
+// (trid_strided_stream.cu); other shapes use adjoint_kernel below.
 // The reference has no adjoint; this is an extension (tridsolver_b200.h).
 #include <cuda_runtime.h>
 
@@ -174,8 +176,42 @@ static tridStatus_t adjoint(const TridParams *ctx, const R *a, const R *b, const
   const Settings &cfg = settings();
   p.flag = pivot_flag_device();
   if (cfg.blocking) pivot_flag_take();
-  // M = 8 rows per thread, T chunks (<= 128), W systems: 64 contiguous bytes
-  // per row when strided, blocks of at most 512 threads
+  // strided batches of 64 < N <= 512 with at least half a 128-byte group of
+  // systems: the streaming kernel in its adjoint form (one pass, 9 words per
+  // element with the products, 5 for dbar alone)
+  if (p.stride > 1 && p.N > 64 && p.N <= 512 && 2 * p.n0 >= (long long)(128 / sizeof(R))) {
+    BatchArgs<R> q{};
+    q.a = a;
+    q.b = b;
+    q.c = c;
+    q.d_in = w;
+    q.d_out = dbar;
+    q.u = prod ? const_cast<R *>(x) : nullptr;
+    q.N = p.N;
+    q.nsys = p.nsys;
+    q.n0 = p.n0;
+    q.st0 = p.st0;
+    q.st1 = p.st1;
+    q.stride = p.stride;
+    q.flag = p.flag;
+    AdjointOut<R> out;
+    out.abar = abar;
+    out.bbar = bbar;
+    out.cbar = cbar;
+    cudaError_t e = p.N <= 128   ? launch_strided_stream_adjoint<R, 4>(q, out, cfg.stream)
+                    : p.N <= 256 ? launch_strided_stream_adjoint<R, 8>(q, out, cfg.stream)
+                                 : launch_strided_stream_adjoint<R, 16>(q, out, cfg.stream);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (e != cudaSuccess) return status_of(e);
+    if (cfg.blocking) {
+      e = cudaStreamSynchronize(cfg.stream);
+      if (e != cudaSuccess) return status_of(e);
+      if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+    }
+    return TRID_STATUS_SUCCESS;
+  }
+  // otherwise M = 8 rows per thread, T chunks (<= 128), W systems: 64
+  // contiguous bytes per row when strided, blocks of at most 512 threads
   const int T = pow2a((p.N + 7) / 8);
   int W = (int)(64 / sizeof(R));
   const int tmax = 512;

@@ -69,6 +69,12 @@ cudaError_t launch_strided_tma(const BatchArgs<R> &p, const Plan &plan, cudaStre
 // Streaming strided kernel (trid_strided_stream.cu): group width for n0
 // systems along the fastest dimension, and its launcher.
 template <typename R> int stream_width(long long n0);
+template <typename R> struct AdjointOut {
+  R *abar = nullptr, *bbar = nullptr, *cbar = nullptr;
+};
+template <typename R, int M>
+cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOut<R> &q,
+                                          cudaStream_t st);
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
 

@@ -29,7 +29,11 @@
 //          x_i = d'_i - a'_i x_first - c'_i x_{i+1}
 //      from the chunk's last row up, and stores.
 // Inc variants carry u through the same window and park it in a third set
-// of private slots until the store. Every element is read once and written
+// of private slots until the store. The adjoint variant solves T^T the same
+// way (c one row up and a one row down as its off-diagonals, w as the right-
+// hand side), parks the forward x in those slots and writes
+// dbar, abar = -dbar x_{i-1}, bbar = -dbar x_i, cbar = -dbar x_{i+1} in the
+// same pass (9 words per element). Every element is read once and written
 // once.
 #include <cuda_runtime.h>
 
@@ -43,30 +47,42 @@ template <typename R> constexpr int stream_w() { return 128 / (int)sizeof(R); }
 template <typename R> constexpr int stream_bs() { return 32 * stream_w<R>(); }
 
 // Row `row` at element offset o: identity rows outside the system, a[0] and
-// c[N-1] forced to zero; u too for Inc.
-template <typename R, bool INC>
+// c[N-1] forced to zero; u too for Inc. The adjoint (ADJ) solves T^T: its
+// sub-diagonal is c one row up and its super-diagonal a one row down, and
+// the fifth value is the forward solution x (in p.u).
+template <typename R, bool FIFTH, int ADJ>
 __device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, long long o, bool valid,
                                                 int row, R &a, R &b, R &c, R &d, R &u) {
   if (valid) {
-    a = row == 0 ? R(0) : __ldg(p.a + o);
+    if constexpr (ADJ) {
+      a = row == 0 ? R(0) : __ldg(p.c + o - p.stride);
+      c = row == p.N - 1 ? R(0) : __ldg(p.a + o + p.stride);
+    } else {
+      a = row == 0 ? R(0) : __ldg(p.a + o);
+      c = row == p.N - 1 ? R(0) : __ldg(p.c + o);
+    }
     b = __ldg(p.b + o);
-    c = row == p.N - 1 ? R(0) : __ldg(p.c + o);
     d = __ldg(p.d_in + o);
-    if constexpr (INC) u = __ldg(p.u + o);
+    if constexpr (FIFTH) u = __ldg(p.u + o);
   } else {
     a = R(0);
     b = R(1);
     c = R(0);
     d = R(0);
-    if constexpr (INC) u = R(0);
+    if constexpr (FIFTH) u = R(0);
   }
 }
 
 }  // namespace
 
-template <typename R, int M, int D, bool SD, int PF, bool INC>
+// ADJ: 0 the forward solve, 1 the adjoint (dbar only), 2 the adjoint with
+// the products abar, bbar, cbar (the forward x is read too).
+template <typename R, int M, int D, bool SD, int PF, bool INC, int ADJ>
 __global__ void __launch_bounds__(stream_bs<R>(), 1)
-    strided_stream_kernel(const BatchArgs<R> p, long long ngx, long long ngroups) {
+    strided_stream_kernel(const BatchArgs<R> p, const AdjointOut<R> q, long long ngx,
+                          long long ngroups) {
+  static_assert(!(INC && ADJ), "Inc or adjoint");
+  constexpr bool FIFTH = INC || ADJ == 2;  // a fifth value per row: u (Inc) or x (adjoint)
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
   static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
   constexpr int W = stream_w<R>();
@@ -79,7 +95,7 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
   R *saf = red + RED + tid;             // a' of row j at [j * BS]
   R *scf = red + RED + M * BS + tid;    // c'
   R *sdf = red + RED + 2 * M * BS + tid;  // d' (SD)
-  R *suf = red + RED + (SD ? 3 : 2) * M * BS + tid;  // u (Inc)
+  R *suf = red + RED + (SD ? 3 : 2) * M * BS + tid;  // u (Inc) or x (adjoint)
   const int s = tid % W;
   const int t = tid / W;
   const int N = p.N;
@@ -98,12 +114,13 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
   // L2 prefetch lanes (PF > 0): lane l < 2 * NA * (32 / W) covers one end
   // (first or last system) of the row segment of one of the NA arrays for
   // one of the warp's chunks
-  constexpr int NA = INC ? 5 : 4;
+  constexpr int NA = FIFTH ? 5 : 4;
   const int lane = tid & 31;
   const bool pf_lane = PF > 0 && lane < 2 * NA * (32 / W);
   const int pq = (lane >> 1) % NA;
   const int pt = (tid >> 5) * (32 / W) + (lane >> 1) / NA;
-  const R *pbase = pq == 0 ? p.a : pq == 1 ? p.b : pq == 2 ? p.c : pq == 3 ? p.d_in : p.u;
+  const R *pbase = pq == 0 ? (ADJ ? p.c : p.a) : pq == 1 ? p.b : pq == 2 ? (ADJ ? p.a : p.c)
+                 : pq == 3 ? p.d_in : p.u;
   auto pf_first = [&](long long g, bool &ok) -> long long {
     const long long gx = g % ngx;
     const long long i1 = g / ngx;
@@ -113,15 +130,15 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     return ok ? i0 * p.st0 + i1 * p.st1 + (long long)pt * M * stride : 0;
   };
 
-  R pa[D], pb[D], pc[D], pd[D], pu[INC ? D : 1];
+  R pa[D], pb[D], pc[D], pd[D], pu[FIFTH ? D : 1];
   long long g = blockIdx.x;
   bool act;
   long long first = group_first(g, act);
   long long lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    stream_load_row<R, INC>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j],
-                            pu[INC ? j : 0]);
+    stream_load_row<R, FIFTH, ADJ>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j],
+                                   pd[j], pu[FIFTH ? j : 0]);
     lo += stride;
   }
   bool pok = false;
@@ -136,6 +153,12 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     bool pokn = false;
     long long pon = 0;
     if constexpr (PF > 0) pon = pf_first(g + gridDim.x, pokn);
+    // adjoint products: the forward x just outside this thread's chunk
+    R xm = R(0), xp = R(0);
+    if constexpr (ADJ == 2) {
+      if (act && row0 >= 1 && row0 - 1 < N) xm = __ldg(p.u + first - stride);
+      if (act && row0 + M <= N - 1) xp = __ldg(p.u + first + (long long)M * stride);
+    }
 
     // forward half of the chunk elimination, streamed row by row
     R rd[SD ? 1 : M];
@@ -144,14 +167,16 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     for (int j = 0; j < M; ++j) {
       const int k = j % D;
       const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
-      if constexpr (INC) suf[j * BS] = pu[k];
+      if constexpr (FIFTH) suf[j * BS] = pu[k];
       if (j + D < M) {
         const int row = row0 + j + D;
-        stream_load_row<R, INC>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k], pu[INC ? k : 0]);
+        stream_load_row<R, FIFTH, ADJ>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k],
+                                       pu[FIFTH ? k : 0]);
         lo += stride;
       } else {
         const int row = row0 + j + D - M;
-        stream_load_row<R, INC>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k], pu[INC ? k : 0]);
+        stream_load_row<R, FIFTH, ADJ>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k],
+                                       pu[FIFTH ? k : 0]);
         ln += stride;
       }
       if constexpr (PF > 0) {
@@ -220,10 +245,20 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
     for (int j = M - 1; j >= 0; --j) {
       if (j < M - 1) x = j == 0 ? y : dval(j) - saf[j * BS] * y - scf[j * BS] * x;
       if (act && row0 + j < N) {
-        if constexpr (INC)
+        if constexpr (INC) {
           p.u[o] = suf[j * BS] + x;
-        else
+        } else {
           p.d_out[o] = x;
+          if constexpr (ADJ == 2) {
+            // abar_i = -dbar_i x_{i-1}, bbar_i = -dbar_i x_i, cbar_i = -dbar_i x_{i+1}
+            const int row = row0 + j;
+            const R xl = j > 0 ? suf[(j - 1) * BS] : xm;
+            const R xr = j < M - 1 ? suf[(j + 1) * BS] : xp;
+            if (q.abar) q.abar[o] = row >= 1 ? -x * xl : R(0);
+            if (q.bbar) q.bbar[o] = -x * suf[j * BS];
+            if (q.cbar) q.cbar[o] = row <= N - 2 ? -x * xr : R(0);
+          }
+        }
       }
       o -= stride;
     }
@@ -258,15 +293,16 @@ template <typename R, int M> constexpr int stream_prefetch() {
   return stream_window<R, M>() >= M ? 0 : sizeof(R) == 8 ? 8 : (M >= 16 ? 12 : M);
 }
 
-template <typename R, int M, bool INC, int PF>
-static cudaError_t launch_stream_pf(const BatchArgs<R> &p, cudaStream_t st) {
+template <typename R, int M, bool INC, int ADJ, int PF>
+static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &q, cudaStream_t st) {
   constexpr int W = stream_w<R>();
   constexpr int BS = stream_bs<R>();
-  constexpr int D = stream_window<R, M>();
+  // the adjoint's window holds 4 rows (an 8-row one spills with the products)
+  constexpr int D = ADJ && stream_window<R, M>() > 4 ? 4 : stream_window<R, M>();
   constexpr bool SD = stream_sd<R, M>();
   const size_t red = ((size_t)6 * 32 * (W + 1) * sizeof(R) + 15) / 16 * 16;
-  const size_t smem = red + (size_t)(2 + (SD ? 1 : 0) + (INC ? 1 : 0)) * M * BS * sizeof(R);
-  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC>;
+  const size_t smem = red + (size_t)(2 + (SD ? 1 : 0) + (INC || ADJ == 2 ? 1 : 0)) * M * BS * sizeof(R);
+  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC, ADJ>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -278,7 +314,7 @@ static cudaError_t launch_stream_pf(const BatchArgs<R> &p, cudaStream_t st) {
     per_sm = 1;
   const long long cap = (long long)sms * per_sm;
   const long long grid = ngroups < cap ? ngroups : cap;
-  kern<<<(unsigned)grid, BS, smem, st>>>(p, ngx, ngroups);
+  kern<<<(unsigned)grid, BS, smem, st>>>(p, q, ngx, ngroups);
   return cudaGetLastError();
 }
 
@@ -287,8 +323,27 @@ cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaS
   if (plan.T != 32 || plan.W != stream_w<R>() || p.N > 32 * M) return cudaErrorInvalidValue;
   constexpr int PF = stream_prefetch<R, M>();
   // L2 prefetch only where the rows of a system are less than 64 KiB apart
-  if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16)) return launch_stream_pf<R, M, INC, PF>(p, st);
-  return launch_stream_pf<R, M, INC, 0>(p, st);
+  const AdjointOut<R> none{};
+  if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
+    return launch_stream_pf<R, M, INC, 0, PF>(p, none, st);
+  return launch_stream_pf<R, M, INC, 0, 0>(p, none, st);
+}
+
+// Adjoint: p.a, p.b, p.c the forward coefficients, p.d_in = w, p.d_out =
+// dbar, p.u = the forward solution x; q the other gradients (any may be
+// null). Same plan rules as the forward solve.
+template <typename R, int M>
+cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOut<R> &q,
+                                          cudaStream_t st) {
+  if (p.N > 32 * M) return cudaErrorInvalidValue;
+  constexpr int PF = stream_prefetch<R, M>();
+  const bool yl = PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16);
+  if (q.abar || q.bbar || q.cbar) {
+    if (yl) return launch_stream_pf<R, M, false, 2, PF>(p, q, st);
+    return launch_stream_pf<R, M, false, 2, 0>(p, q, st);
+  }
+  if (yl) return launch_stream_pf<R, M, false, 1, PF>(p, q, st);
+  return launch_stream_pf<R, M, false, 1, 0>(p, q, st);
 }
 
 #define INST_STREAM(R, M)                                                                       \
@@ -296,6 +351,15 @@ cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaS
                                                            cudaStream_t);                      \
   template cudaError_t launch_strided_stream<R, M, true>(const BatchArgs<R> &, const Plan &,     \
                                                           cudaStream_t);
+#define INST_STREAM_ADJ(R, M)                                                                   \
+  template cudaError_t launch_strided_stream_adjoint<R, M>(const BatchArgs<R> &,                  \
+                                                           const AdjointOut<R> &, cudaStream_t);
+INST_STREAM_ADJ(double, 4)
+INST_STREAM_ADJ(double, 8)
+INST_STREAM_ADJ(double, 16)
+INST_STREAM_ADJ(float, 4)
+INST_STREAM_ADJ(float, 8)
+INST_STREAM_ADJ(float, 16)
 INST_STREAM(double, 4)
 INST_STREAM(double, 8)
 INST_STREAM(double, 16)
