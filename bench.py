@@ -48,7 +48,7 @@ def parse_args():
     ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--only-config", default=None,
-                    choices=["sweep", "adi", "precision", "ragged", "adjoint"],
+                    choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint"],
                     help="run just one of the other configurations and print its JSON (profiling)")
     ap.add_argument("--ragged-systems", type=int, default=200000,
                     help="systems in the ragged configuration (200000 = the benchmark)")
@@ -636,6 +636,7 @@ def main():
         hbm = peaks()[0]
         grid = [int(v) for v in args.grid.split(",")] if args.grid else None
         fn = {"sweep": lambda: config_sweep(dev, hbm), "adi": lambda: config_adi(dev, hbm),
+              "adi_f32": lambda: config_adi(dev, hbm, (128, 512, 512), 1000, "f32"),
               "precision": lambda: config_precision(dev, args.n, grid),
               "ragged": lambda: config_ragged(dev, hbm, args.ragged_systems),
               "adjoint": lambda: config_adjoint(dev)}[args.only_config]
