@@ -431,36 +431,47 @@ def config_sweep(dev, hbm):
 
 
 def config_adi(dev, hbm, n=(256, 256, 256), steps=100, dtype="f64", alpha=1.0):
-    """ADI heat steps replayed from a CUDA graph of one timestep."""
+    """ADI heat steps replayed from a CUDA graph of one timestep, in the fused
+    form (coefficients as scalars, stencil inside the x solve: 7 words per
+    point and step) and in the reference application's form (coefficient
+    arrays: 21 words)."""
     import numpy as np
     import torch
     from tridsolver_b200.adi import ADIHeat
     dt = torch.float64 if dtype == "f64" else torch.float32
     es = 8 if dtype == "f64" else 4
     nz, ny, nx = n
-    g = torch.Generator(device=dev).manual_seed(3)
-    u = torch.randn((nz, ny, nx), generator=g, device=dev, dtype=dt)
-    u[0], u[-1], u[:, 0], u[:, -1], u[:, :, 0], u[:, :, -1] = 0, 0, 0, 0, 0, 0
-    lams = np.random.default_rng(4).uniform(0.1, 1.0, steps + 2)
-    sim = ADIHeat(u, lams, alpha=alpha)
-    sim.capture()
-    sim.reset_counter(0)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    sim.run(steps)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
     elems = nx * ny * nz
-    words = 5 + 5 + 5 + 6  # RHS+coefficients, x, y, z-Inc (one shared coefficient set)
-    gbs = words * es * elems / ms / 1e6
-    return {"grid": [nx, ny, nz], "dtype": dtype, "steps": steps, "ms_per_step": round(ms, 4),
-            "elements_per_s": elems / ms * 1e3, "hbm_gbs": round(gbs, 1),
-            "frac": round(gbs / hbm, 4), "words_per_element_step": words,
-            "graph": "one timestep captured, replayed per step; lambda[step] read on the device",
-            "finite": bool(torch.isfinite(sim.u).all().item())}
+    out = {"grid": [nx, ny, nz], "dtype": dtype, "steps": steps,
+           "graph": "one timestep captured, replayed per step; lambda[step] read on the device"}
+    for form, arrays, words in (("fused", False, 7), ("arrays", True, 5 + 5 + 5 + 6)):
+        g = torch.Generator(device=dev).manual_seed(3)
+        u = torch.randn((nz, ny, nx), generator=g, device=dev, dtype=dt)
+        u[0], u[-1], u[:, 0], u[:, -1], u[:, :, 0], u[:, :, -1] = 0, 0, 0, 0, 0, 0
+        lams = np.random.default_rng(4).uniform(0.1, 1.0, steps + 2)
+        sim = ADIHeat(u, lams, alpha=alpha, coefficient_arrays=arrays)
+        sim.capture()
+        sim.reset_counter(0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.run(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        gbs = words * es * elems / ms / 1e6
+        out[form] = {"ms_per_step": round(ms, 4), "elements_per_s": elems / ms * 1e3,
+                     "hbm_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
+                     "words_per_element_step": words,
+                     "finite": bool(torch.isfinite(sim.u).all().item())}
+        if form == "fused":
+            u_fused = sim.u.clone()
+        else:
+            out["fused_vs_arrays_max_abs"] = float((u_fused - sim.u).abs().max().item())
+        del sim, u
+        torch.cuda.empty_cache()
+    return out
 
 
 def config_precision(dev, n=512, dims=None):

@@ -12,8 +12,11 @@
 // lambda is read on the device from lam[*step] (lam[0] when step is NULL), and
 // *step is advanced by one at the end of the timestep, so a captured CUDA
 // graph of one timestep replays a sequence of per-step lambdas. The reference
-// writes nine coefficient arrays (x, y and z copies of identical values); the
-// three directions here share one set.
+// writes nine coefficient arrays (x, y and z copies of identical values). With
+// a, b, c given, the three directions here share one set (a preprocessing
+// kernel and three array solves, 21 words of traffic per point); with a, b, c
+// all NULL the coefficients stay three scalars and the stencil is fused into
+// the x solve (three kernels, 7 words per point).
 #include <cuda_runtime.h>
 
 #include "trid_internal.h"
@@ -58,10 +61,43 @@ __global__ void adi_advance_kernel(int *step) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
 
+// The fused timestep: x solve with the stencil, y solve, z solve into u.
+template <typename R>
+static cudaError_t adi_fused(R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx, int ny,
+                             int nz, cudaStream_t st) {
+  cudaError_t e = launch_adi_x<R>(u, du, k, flag, nx, ny, nz, st);
+  if (e != cudaSuccess) return e;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  BatchArgs<R> p{};
+  p.d_in = du;
+  p.d_out = du;
+  p.flag = flag;
+  p.n0 = nx;
+  p.st0 = 1;
+  // y: systems (x, z), rows nx apart
+  p.N = ny;
+  p.nsys = (long long)nx * nz;
+  p.st1 = (long long)nx * ny;
+  p.stride = nx;
+  e = launch_adi_yz<R, false>(p, k, st);
+  if (e != cudaSuccess) return e;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  // z: systems (x, y), rows a plane apart, u += x
+  p.u = u;
+  p.N = nz;
+  p.nsys = (long long)nx * ny;
+  p.st1 = nx;
+  p.stride = (long long)nx * ny;
+  e = launch_adi_yz<R, true>(p, k, st);
+  if (e == cudaSuccess) g_launches.fetch_add(1, std::memory_order_relaxed);
+  return e;
+}
+
 template <typename R>
 static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *step, R alpha,
                              int nx, int ny, int nz) {
-  if (!u || !du || !a || !b || !c || !lam || nx < 1 || ny < 1 || nz < 1)
+  const bool arrays = a || b || c;
+  if (!u || !du || !lam || nx < 1 || ny < 1 || nz < 1 || (arrays && (!a || !b || !c)))
     return TRID_STATUS_INVALID_VALUE;
   int dev = 0, major = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -75,13 +111,28 @@ static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *s
   unsigned *flag = pivot_flag_device();
   if (cfg.blocking) pivot_flag_take();
   const long long n = (long long)nx * ny * nz;
+  cudaError_t e = cudaSuccess;
+  R *scratch = nullptr;
+  if (!arrays && nx <= 512 && ny <= 512 && nz <= 512) {
+    e = adi_fused<R>(u, du, ConstCoef<R>{lam, step, alpha}, flag, nx, ny, nz, st);
+    goto advance;
+  }
+  if (!arrays) {
+    // longer systems: the array path on pool scratch
+    e = scratch_alloc((void **)&scratch, (size_t)3 * n * sizeof(R), st);
+    if (e != cudaSuccess) return status_of(e);
+    a = scratch;
+    b = scratch + n;
+    c = scratch + 2 * n;
+  }
+  {
   const int threads = 256;
   long long blocks = (n + threads - 1) / threads;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   adi_preproc_kernel<R><<<(unsigned)blocks, threads, 0, st>>>(u, du, a, b, c, lam, step, alpha, nx, ny,
                                                             nz);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   const long long dims[3] = {nx, ny, nz};
   for (int sd = 0; sd < 3 && e == cudaSuccess; ++sd) {
     BatchArgs<R> p{};
@@ -115,6 +166,12 @@ static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *s
     const Plan plan = choose_plan<R>(p, vec_aligned<R>(p), false);
     e = sd == 2 ? launch_batch<R, true>(p, plan, st) : launch_batch<R, false>(p, plan, st);
   }
+  }
+  if (scratch) {
+    const cudaError_t ef = scratch_free(scratch, st);
+    if (e == cudaSuccess) e = ef;
+  }
+advance:
   if (e == cudaSuccess && step) {
     adi_advance_kernel<<<1, 32, 0, st>>>(step);
     g_launches.fetch_add(1, std::memory_order_relaxed);

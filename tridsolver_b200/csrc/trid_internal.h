@@ -78,6 +78,15 @@ cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOu
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
 
+// Solves of the fused ADI timestep (trid_adi_fused.cu): the x solve with the
+// 7-point stencil of u formed on the fly (du written), 1 <= nx <= 512; the y
+// or z solve of du in place (INC: u += solution), 1 <= N <= 512.
+template <typename R>
+cudaError_t launch_adi_x(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx, int ny,
+                         int nz, cudaStream_t st);
+template <typename R, bool INC>
+cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st);
+
 // Whether every pointer and every system start allows 16-byte vector access
 // (contiguous systems only).
 template <typename R>

@@ -43,6 +43,25 @@ template <typename R> struct BatchArgs {
   unsigned *flag;  // host-mapped zero-pivot word (may be null)
 };
 
+// Constant coefficients of one ADI heat timestep, read on the device:
+// lambda = lam[*step] (lam[0] when step is null) and, on interior rows of
+// systems through the grid's interior,
+//     a = c = -alpha * lambda,  b = 1 + 2 * alpha * lambda;
+// identity rows (a = c = 0, b = 1) everywhere else (the coefficient arrays
+// of apps/adi/src/preproc.cu:40-90, as three scalars and a boundary test).
+template <typename R> struct ConstCoef {
+  const R *lam;
+  const int *step;
+  R alpha;
+};
+
+template <typename R>
+__device__ __forceinline__ void const_coef(const ConstCoef<R> &k, R &l, R &ca, R &cb) {
+  l = k.lam[k.step ? *k.step : 0];
+  ca = -k.alpha * l;
+  cb = R(1) + R(2) * k.alpha * l;
+}
+
 template <typename R>
 __device__ __forceinline__ long long sys_base(const BatchArgs<R> &p, long long s) {
   long long i1 = s / p.n0;
