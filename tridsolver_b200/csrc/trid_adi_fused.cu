@@ -15,12 +15,14 @@
 // substitution, no reciprocals. Identity systems off the interior are
 // neither read nor written (their solution is their zero right-hand side).
 //
-// Because the right-hand-side arithmetic is the array kernels' operation for
-// operation, the results equal the coefficient-array timestep's where both
-// use the same chunking:
+// The right-hand-side arithmetic is the array kernels' operation for
+// operation, so where both use the same chunking the results agree with the
+// coefficient-array timestep's to rounding (the kernels' instruction
+// selection, i.e. which products fuse into multiply-adds, may differ):
 //   adi_x_kernel      mirrors contig_smem_kernel (chunk_forward,
 //                     chunk_backward, reduced_solve, chunk_substitute), with
-//                     the 7-point stencil formed while the line is staged;
+//                     the 7-point stencil formed from planes of u staged in
+//                     shared memory;
 //   adi_stream_kernel mirrors strided_stream_kernel (forward sweep, one-row
 //                     backward recursion, block-wide reduced solve,
 //                     back-substitution from the forward rows).
@@ -35,10 +37,17 @@ namespace {
 constexpr int kT = 32;      // chunks per system (one warp of reduced rows)
 constexpr int kSteps = 5;   // cyclic-reduction steps over 32 reduced rows
 
+// Two table entries read with one vector load.
+template <typename R> struct alignas(2 * sizeof(R)) Pair {
+  R x, y;
+};
+
 // Coefficients of the reduced system's solve (reduced_solve) by lane = chunk.
 template <typename R> struct PcrTab {
-  R tA[kT], tC[kT], bA[kT], bC[kT], ri[kT];
-  R al[kSteps][kT], ga[kSteps][kT], rs[kSteps][kT];
+  Pair<R> tAC[kT], bAC[kT];  // (A, C) of the top and bottom reduced rows
+  R ri[kT];
+  Pair<R> alga[kSteps][kT];  // (alpha, gamma) before each step
+  R rs[kSteps][kT];
 };
 
 // The coefficient half of reduced_solve for the chunk rows of lane t:
@@ -46,10 +55,8 @@ template <typename R> struct PcrTab {
 // Every lane of the warp calls this.
 template <typename R>
 __device__ void pcr_factor(PcrTab<R> &q, R tA, R tC, R bA, R bC, int t, bool &bad) {
-  q.tA[t] = tA;
-  q.tC[t] = tC;
-  q.bA[t] = bA;
-  q.bC[t] = bC;
+  q.tAC[t] = Pair<R>{tA, tC};
+  q.bAC[t] = Pair<R>{bA, bC};
   R pA = shfl_up(bA, 1, kT);
   R pC = shfl_up(bC, 1, kT);
   if (t == 0) {
@@ -77,8 +84,7 @@ __device__ void pcr_factor(PcrTab<R> &q, R tA, R tC, R bA, R bC, int t, bool &ba
       al_r = R(0);
       ga_r = R(0);
     }
-    q.al[k][t] = al;
-    q.ga[k][t] = ga;
+    q.alga[k][t] = Pair<R>{al, ga};
     R b2 = R(1) - al * ga_l - ga * al_r;
     R a2 = -al * al_l;
     R g2 = -ga * ga_r;
@@ -97,7 +103,8 @@ template <typename R>
 __device__ __forceinline__ void pcr_solve_d(const PcrTab<R> &q, R tD, R bD, int t, R &y, R &z) {
   R pD = shfl_up(bD, 1, kT);
   if (t == 0) pD = R(0);
-  R de = tD - q.tA[t] * pD - q.tC[t] * bD;
+  const Pair<R> tp = q.tAC[t];
+  R de = tD - tp.x * pD - tp.y * bD;
   de *= q.ri[t];
   int k = 0;
 #pragma unroll
@@ -105,13 +112,15 @@ __device__ __forceinline__ void pcr_solve_d(const PcrTab<R> &q, R tD, R bD, int 
     R de_l = shfl_up(de, s, kT), de_r = shfl_down(de, s, kT);
     if (t < s) de_l = R(0);
     if (t + s >= kT) de_r = R(0);
-    R d2 = de - q.al[k][t] * de_l - q.ga[k][t] * de_r;
+    const Pair<R> ag = q.alga[k][t];
+    R d2 = de - ag.x * de_l - ag.y * de_r;
     de = d2 * q.rs[k][t];
   }
   y = de;
   R yn = shfl_down(y, 1, kT);
   if (t == kT - 1) yn = R(0);
-  z = bD - q.bA[t] * y - q.bC[t] * yn;
+  const Pair<R> bp = q.bAC[t];
+  z = bD - bp.x * y - bp.y * yn;
 }
 
 // Row `row` of a system of N rows: interior rows carry the constant
@@ -124,31 +133,42 @@ __device__ __forceinline__ void cc_row(int row, int N, R ca, R cb, R &a, R &b) {
 }
 
 // ---- contiguous form (chunk_forward / chunk_backward / chunk_substitute) ----
+//
+// A chunk's elimination depends only on its own rows, so the 32 chunks of a
+// line fall into four classes with equal factors: the first (row 0 is an
+// identity row), the interior ones, the one holding row N-1, and those past
+// N (identity rows only). The chunk tables are kept per class, so the lanes
+// of a warp read them mostly from one address (a broadcast); the reduced
+// solve's tables stay per lane.
+
+__device__ __forceinline__ int chunk_class(int t, int N, int M) {
+  const int tl = (N - 1) / M;  // chunk holding row N-1
+  return t == 0 ? 0 : t < tl ? 1 : t == tl ? 2 : 3;
+}
 
 template <typename R, int M> struct ContigTab {
-  R r[M][kT];   // forward reciprocal pivots
-  R ao[M][kT];  // unscaled sub-diagonal
-  R cF[M][kT];  // super-diagonal after the forward half
-  R aB[M][kT];  // after the backward half
-  R cB[M][kT];
-  R rb[kT];     // reciprocal of the backward half's top-row pivot
+  Pair<R> rao[4][M];  // (forward reciprocal pivot, unscaled sub-diagonal)
+  R cF[4][M];         // super-diagonal after the forward half
+  Pair<R> acB[4][M];  // (a, c) after the backward half
+  R rb[4];            // reciprocal of the backward half's top-row pivot
   PcrTab<R> pcr;
 };
 
+// Lane t factors chunk t; the lanes of one class store equal values.
 template <typename R, int M>
 __device__ void contig_factor(ContigTab<R, M> &f, R ca, R cb, int N, int t, bool &bad) {
+  const int cl = chunk_class(t, N, M);
   R a[M], b[M], c[M];
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     cc_row<R>(t * M + i, N, ca, cb, a[i], b[i]);
     c[i] = a[i];
-    f.ao[i][t] = a[i];
   }
 #pragma unroll
   for (int i = 0; i < (M < 2 ? M : 2); ++i) {
     R r = rcp(b[i]);
     bad |= !finite_rcp(r);
-    f.r[i][t] = r;
+    f.rao[cl][i] = Pair<R>{r, a[i]};
     a[i] *= r;
     c[i] *= r;
   }
@@ -156,12 +176,12 @@ __device__ void contig_factor(ContigTab<R, M> &f, R ca, R cb, int N, int t, bool
   for (int i = 2; i < M; ++i) {
     R r = rcp(b[i] - a[i] * c[i - 1]);
     bad |= !finite_rcp(r);
-    f.r[i][t] = r;
+    f.rao[cl][i] = Pair<R>{r, a[i]};
     a[i] = -r * a[i] * a[i - 1];
     c[i] = r * c[i];
   }
 #pragma unroll
-  for (int i = 0; i < M; ++i) f.cF[i][t] = c[i];
+  for (int i = 0; i < M; ++i) f.cF[cl][i] = c[i];
 #pragma unroll
   for (int i = M - 3; i >= 1; --i) {
     a[i] = a[i] - c[i] * a[i + 1];
@@ -174,41 +194,101 @@ __device__ void contig_factor(ContigTab<R, M> &f, R ca, R cb, int N, int t, bool
     a[0] = rb * a[0];
     c[0] = -rb * c[0] * c[1];
   }
-  f.rb[t] = rb;
+  f.rb[cl] = rb;
 #pragma unroll
-  for (int i = 0; i < M; ++i) {
-    f.aB[i][t] = a[i];
-    f.cB[i][t] = c[i];
-  }
+  for (int i = 0; i < M; ++i) f.acB[cl][i] = Pair<R>{a[i], c[i]};
   pcr_factor<R>(f.pcr, a[0], c[0], a[M - 1], c[M - 1], t, bad);
 }
 
-// x solve of one line held by a warp (lane t = chunk t), in place in d.
+// x solves of two lines held by a warp (lane t = chunk t of class cl), in
+// place in d0 and d1; every table value is read once for both.
 template <typename R, int M>
-__device__ __forceinline__ void contig_solve_d(const ContigTab<R, M> &f, R (&d)[M], int t) {
+__device__ __forceinline__ void contig_solve_d2(const ContigTab<R, M> &f, R (&d0)[M], R (&d1)[M],
+                                                int t, int cl) {
 #pragma unroll
-  for (int i = 0; i < (M < 2 ? M : 2); ++i) d[i] *= f.r[i][t];
+  for (int i = 0; i < (M < 2 ? M : 2); ++i) {
+    const R r = f.rao[cl][i].x;
+    d0[i] *= r;
+    d1[i] *= r;
+  }
 #pragma unroll
-  for (int i = 2; i < M; ++i) d[i] = f.r[i][t] * (d[i] - f.ao[i][t] * d[i - 1]);
+  for (int i = 2; i < M; ++i) {
+    const Pair<R> ra = f.rao[cl][i];
+    d0[i] = ra.x * (d0[i] - ra.y * d0[i - 1]);
+    d1[i] = ra.x * (d1[i] - ra.y * d1[i - 1]);
+  }
 #pragma unroll
-  for (int i = M - 3; i >= 1; --i) d[i] = d[i] - f.cF[i][t] * d[i + 1];
-  if (M >= 3) d[0] = f.rb[t] * (d[0] - f.cF[0][t] * d[1]);
-  R y, z;
-  pcr_solve_d<R>(f.pcr, d[0], d[M - 1], t, y, z);
+  for (int i = M - 3; i >= 1; --i) {
+    const R cfw = f.cF[cl][i];
+    d0[i] = d0[i] - cfw * d0[i + 1];
+    d1[i] = d1[i] - cfw * d1[i + 1];
+  }
+  if (M >= 3) {
+    const R rb = f.rb[cl], c0 = f.cF[cl][0];
+    d0[0] = rb * (d0[0] - c0 * d0[1]);
+    d1[0] = rb * (d1[0] - c0 * d1[1]);
+  }
+  // reduced solves of both lines, step by step
+  const PcrTab<R> &q = f.pcr;
+  R p0 = shfl_up(d0[M - 1], 1, kT), p1 = shfl_up(d1[M - 1], 1, kT);
+  if (t == 0) {
+    p0 = R(0);
+    p1 = R(0);
+  }
+  const Pair<R> tp = q.tAC[t];
+  const R ri = q.ri[t];
+  R e0 = d0[0] - tp.x * p0 - tp.y * d0[M - 1];
+  R e1 = d1[0] - tp.x * p1 - tp.y * d1[M - 1];
+  e0 *= ri;
+  e1 *= ri;
+  int k = 0;
 #pragma unroll
-  for (int i = 1; i < M - 1; ++i) d[i] = d[i] - f.aB[i][t] * y - f.cB[i][t] * z;
-  d[0] = y;
-  if (M > 1) d[M - 1] = z;
+  for (int s = 1; s < kT; s <<= 1, ++k) {
+    R l0 = shfl_up(e0, s, kT), r0 = shfl_down(e0, s, kT);
+    R l1 = shfl_up(e1, s, kT), r1 = shfl_down(e1, s, kT);
+    if (t < s) {
+      l0 = R(0);
+      l1 = R(0);
+    }
+    if (t + s >= kT) {
+      r0 = R(0);
+      r1 = R(0);
+    }
+    const Pair<R> ag = q.alga[k][t];
+    const R rs = q.rs[k][t];
+    R g0 = e0 - ag.x * l0 - ag.y * r0;
+    R g1 = e1 - ag.x * l1 - ag.y * r1;
+    e0 = g0 * rs;
+    e1 = g1 * rs;
+  }
+  R n0 = shfl_down(e0, 1, kT), n1 = shfl_down(e1, 1, kT);
+  if (t == kT - 1) {
+    n0 = R(0);
+    n1 = R(0);
+  }
+  const Pair<R> bp = q.bAC[t];
+  const R z0 = d0[M - 1] - bp.x * e0 - bp.y * n0;
+  const R z1 = d1[M - 1] - bp.x * e1 - bp.y * n1;
+#pragma unroll
+  for (int i = 1; i < M - 1; ++i) {
+    const Pair<R> ac = f.acB[cl][i];
+    d0[i] = d0[i] - ac.x * e0 - ac.y * z0;
+    d1[i] = d1[i] - ac.x * e1 - ac.y * z1;
+  }
+  d0[0] = e0;
+  d1[0] = e1;
+  if (M > 1) {
+    d0[M - 1] = z0;
+    d1[M - 1] = z1;
+  }
 }
 
 // ---- streaming form (strided_stream_kernel) --------------------------------
 
 template <typename R, int M> struct StreamTab {
-  R r[M][kT];   // forward reciprocal pivots
-  R ao[M][kT];  // unscaled sub-diagonal
-  R af[M][kT];  // forward a'
-  R cf[M][kT];  // forward c'
-  R r0[kT];     // reciprocal of the top reduced row's pivot
+  Pair<R> rao[M][kT];  // (forward reciprocal pivot, unscaled sub-diagonal)
+  Pair<R> acf[M][kT];  // forward (a', c')
+  R r0[kT];            // reciprocal of the top reduced row's pivot
   PcrTab<R> pcr;
 };
 
@@ -232,10 +312,8 @@ __device__ void stream_factor(StreamTab<R, M> &f, R ca, R cb, int N, int t, bool
       cf = r * c;
     }
     bad |= !finite_rcp(r);
-    f.r[j][t] = r;
-    f.ao[j][t] = a;
-    f.af[j][t] = af;
-    f.cf[j][t] = cf;
+    f.rao[j][t] = Pair<R>{r, a};
+    f.acf[j][t] = Pair<R>{af, cf};
     afv[j] = af;
     cfv[j] = cf;
     ap = af;
@@ -255,127 +333,237 @@ __device__ void stream_factor(StreamTab<R, M> &f, R ca, R cb, int N, int t, bool
   pcr_factor<R>(f.pcr, r0 * a0, -r0 * c0 * C, ap, cp, t, bad);
 }
 
+// A line of 32 chunk rows of M elements in shared memory without padding:
+// its 16-byte units are permuted within each chunk row (unit u is stored at
+// u ^ ((u >> 3) & (UPR - 1)), UPR units per chunk row) so that the eight
+// lanes of a quarter warp, reading unit q of their own chunk rows, hit eight
+// different 16-byte bank groups.
+template <typename R, int M> struct SwzLine {
+  static constexpr int VN = 16 / (int)sizeof(R);  // elements per unit
+  static constexpr int UPR = M / VN;               // units per chunk row
+  static constexpr int LEN = 32 * M;               // elements per line
+  static_assert(UPR == 2 || UPR == 4 || UPR == 8, "2, 4 or 8 units per chunk row");
+  __device__ static __forceinline__ int unit(int u) { return u ^ ((u >> 3) & (UPR - 1)); }
+  __device__ static __forceinline__ int idx(int e) { return unit(e / VN) * VN + e % VN; }
+};
+
+// Chunk row `lane` of a swizzled line into registers, and back.
+template <typename R, int M>
+__device__ __forceinline__ void lds_swz(const R *line, int lane, R (&v)[M]) {
+  using S = SwzLine<R, M>;
+  using Vt = typename Vec16<R>::T;
+#pragma unroll
+  for (int q = 0; q < S::UPR; ++q) {
+    const Vt x = *reinterpret_cast<const Vt *>(line + S::unit(S::UPR * lane + q) * S::VN);
+#pragma unroll
+    for (int i = 0; i < S::VN; ++i) v[q * S::VN + i] = reinterpret_cast<const R *>(&x)[i];
+  }
+}
+template <typename R, int M>
+__device__ __forceinline__ void sts_swz(R *line, int lane, const R (&v)[M]) {
+  using S = SwzLine<R, M>;
+  using Vt = typename Vec16<R>::T;
+#pragma unroll
+  for (int q = 0; q < S::UPR; ++q) {
+    Vt x;
+#pragma unroll
+    for (int i = 0; i < S::VN; ++i) reinterpret_cast<R *>(&x)[i] = v[q * S::VN + i];
+    *reinterpret_cast<Vt *>(line + S::unit(S::UPR * lane + q) * S::VN) = x;
+  }
+}
+
 template <typename R> constexpr int adi_w() { return 128 / (int)sizeof(R); }
 template <typename R> constexpr int adi_bs() { return kT * adi_w<R>(); }
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// x solve with the stencil. A persistent CTA of NW warps; each warp takes x
-// lines (j, k) in turn. The right-hand side of a line is formed while it is
-// staged: each lane takes V-element units (16 bytes when the lines are
-// 16-byte aligned) of the line and of its neighbour lines j +- 1, k +- 1
-// (which the warps of those lines read too, so mostly from L2), sums the
-// 7-point stencil in the order of adi_preproc_kernel and parks du in the
-// warp's padded shared-memory line; lane t then reads its chunk row.
-template <typename R, int M, bool VEC, int NW>
-__global__ void __launch_bounds__(NW * 32) adi_x_kernel(const R *__restrict__ u, R *__restrict__ du,
-                                                        const ConstCoef<R> k, unsigned *flag,
-                                                        int nx, int ny, int nz) {
-  using L = SmemLayout<R, M>;
-  constexpr int V = VEC ? L::V : 1;
-  constexpr int UPL = M / V;  // units per lane (nx <= 32 M)
+// x solve with the stencil, marching along z. A CTA of J / 2 warps owns a
+// tile of J consecutive x lines (j0 .. j0+J-1) and walks it through a range
+// of planes k. The planes' slabs of J + 2 lines (the tile and its j +- 1
+// halo) stream through a ring of LA + 3 slabs in shared memory with
+// cp.async, LA planes ahead of the one being solved, so u crosses L2 about
+// once per element instead of five times. Warp w forms the 7-point
+// right-hand sides of lines j0 + 2w and j0 + 2w + 1 of plane k from the
+// slabs of planes k - 1, k, k + 1 (in the order of adi_preproc_kernel; each
+// line is the other's j neighbour), solves both with the factored
+// coefficients (lane t = chunk t), and stores them through its own line
+// buffers, so the global stores are coalesced. Lines in shared memory use
+// the swizzled layout of SwzLine (no padding; the lanes' 16-byte chunk reads
+// are free of bank conflicts).
+//
+// Work: the (tile, plane) steps, tile-major, are split evenly over the grid
+// (one CTA per SM); a CTA whose range crosses into the next tile restarts
+// its ring there.
+template <typename R, int M, bool VEC, int J, int LA>
+__global__ void __launch_bounds__(J * 16, 1)
+    adi_x_kernel(const R *__restrict__ u, R *__restrict__ du, const ConstCoef<R> k, unsigned *flag,
+                 int nx, int ny, int nz, int jtiles) {
+  static_assert(J % 2 == 0, "two lines per warp");
+  using S = SwzLine<R, M>;
+  constexpr int LB = S::LEN;           // elements per line buffer
+  constexpr int V = VEC ? S::VN : 1;  // elements per copy unit
+  constexpr int NS = LA + 3;           // slabs in the ring
+  constexpr int SL = J + 2;            // lines per slab
+  constexpr int NT = J * 16;           // threads
   using Vt = typename Vec16<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ContigTab<R, M> &f = *reinterpret_cast<ContigTab<R, M> *>(smem_raw);
+  R *ring = reinterpret_cast<R *>(smem_raw + (sizeof(ContigTab<R, M>) + 15) / 16 * 16);
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  R *buf = reinterpret_cast<R *>(smem_raw + (sizeof(ContigTab<R, M>) + 15) / 16 * 16) + warp * L::BUF;
+  R *outb = ring + NS * SL * LB + 2 * warp * LB;  // two line buffers per warp
   R l, ca, cb;
   const_coef<R>(k, l, ca, cb);
   bool bad = false;
   if (warp == 0) contig_factor<R, M>(f, ca, cb, nx, lane, bad);
-  __syncthreads();
-  const long long nlines = (long long)ny * nz;
-  const long long nxy = (long long)nx * ny;
+  const int cl = chunk_class(lane, nx, M);
   const int nunits = (nx + V - 1) / V;
-  for (long long line = (long long)blockIdx.x * NW + warp; line < nlines;
-       line += (long long)gridDim.x * NW) {
-    const long long kz = line / ny;
-    const long long jy = line - kz * ny;
-    R *dst = du + line * nx;
-    if (jy == 0 || jy == ny - 1 || kz == 0 || kz == nz - 1) {
+  const long long plane = (long long)nx * ny;
+  const long long total = (long long)jtiles * nz;
+  const long long s0 = total * blockIdx.x / gridDim.x;
+  const long long s1 = total * (blockIdx.x + 1) / gridDim.x;
+
+  // this thread's copy units of a slab (the same for every plane of a tile):
+  // element offset in the plane and in the slab, -1 where there is none
+  constexpr int UQ = ((J + 2) * 32 * (M / V) + NT - 1) / NT;
+  int goff[UQ], soff[UQ];
+  auto set_tile = [&](int jt) {
+    const int jlo = jt * J - 1;
 #pragma unroll
-      for (int q = 0; q < UPL; ++q) {
-        const int un = lane + 32 * q;
-        const int e = un * V;
-        if (un >= nunits) break;
-        if (VEC && e + V <= nx) {
-          Vt zv;
-          R *zs = reinterpret_cast<R *>(&zv);
-#pragma unroll
-          for (int i = 0; i < L::V; ++i) zs[i] = R(0);
-          *reinterpret_cast<Vt *>(dst + e) = zv;
-        } else {
-          for (int i = 0; i < V && e + i < nx; ++i) dst[e + i] = R(0);
-        }
-      }
-      continue;
-    }
-    const R *c0 = u + line * nx;
-    const R *nb[4] = {c0 - nx, c0 + nx, c0 - nxy, c0 + nxy};
-#pragma unroll
-    for (int q = 0; q < UPL; ++q) {
-      const int un = lane + 32 * q;
+    for (int q = 0; q < UQ; ++q) {
+      const int idx = threadIdx.x + q * NT;
+      const int ll = idx / nunits;
+      const int un = idx - ll * nunits;
+      const int jj = jlo + ll;
       const int e = un * V;
-      if (un < nunits) {
-        R cv[V], s6[V];
-        if (VEC && e + V <= nx) {
-          const Vt x = __ldg(reinterpret_cast<const Vt *>(c0 + e));
+      const bool ok = ll < SL && jj >= 0 && jj < ny;
+      goff[q] = ok ? jj * nx + e : -1;
+      soff[q] = ok ? ll * LB + S::idx(e) : -1;
+    }
+  };
+  // slab of plane kp into its ring slot (planes kb - 1 .. ke of the segment
+  // [kb, ke) only); always closes a copy group
+  auto load_plane = [&](int kp, int kb, int ke) {
+    if (kp >= 0 && kp < nz && kp <= ke) {
+      R *slab = ring + ((kp - kb + 1) % NS) * SL * LB;
+      const R *src = u + (long long)kp * plane;
 #pragma unroll
-          for (int i = 0; i < V; ++i) cv[i] = reinterpret_cast<const R *>(&x)[i];
-        } else {
-#pragma unroll
-          for (int i = 0; i < V; ++i) cv[i] = e + i < nx ? __ldg(c0 + e + i) : R(0);
-        }
-        const R left = e > 0 ? __ldg(c0 + e - 1) : R(0);
-        const R right = e + V < nx ? __ldg(c0 + e + V) : R(0);
-#pragma unroll
-        for (int i = 0; i < V; ++i)
-          s6[i] = (i == 0 ? left : cv[i - 1]) + (i == V - 1 ? right : cv[i + 1]);
-#pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          if (VEC && e + V <= nx) {
-            const Vt x = __ldg(reinterpret_cast<const Vt *>(nb[n] + e));
-#pragma unroll
-            for (int i = 0; i < V; ++i) s6[i] = s6[i] + reinterpret_cast<const R *>(&x)[i];
-          } else {
-#pragma unroll
-            for (int i = 0; i < V; ++i)
-              if (e + i < nx) s6[i] = s6[i] + __ldg(nb[n] + e + i);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-          const int x = e + i;
-          if (x < nx) buf[x + (x / M) * L::V] = (x >= 1 && x <= nx - 2) ? l * (s6[i] - R(6) * cv[i]) : R(0);
+      for (int q = 0; q < UQ; ++q) {
+        if (soff[q] >= 0) {
+          if constexpr (VEC)
+            cp_async16(slab + soff[q], src + goff[q], 16);
+          else
+            cp_async_elem<R>(slab + soff[q], src + goff[q]);
         }
       }
     }
-    __syncwarp();
-    R rd[M];
-    lds_row<R, M>(buf + lane * L::ROW, rd);
-#pragma unroll
-    for (int i = 0; i < M; ++i)
-      if (lane * M + i >= nx) rd[i] = R(0);
-    contig_solve_d<R, M>(f, rd, lane);
-    __syncwarp();  // every lane has read its row before any row is rewritten
-    sts_row<R, M>(buf + lane * L::ROW, rd);
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < UPL; ++q) {
-      const int un = lane + 32 * q;
+    cp_async_commit();
+  };
+  // stores line buffer ob to global line dst (zeros when `zero`)
+  auto store_line = [&](R *dst, const R *ob, bool zero) {
+    for (int un = lane; un < nunits; un += 32) {
       const int e = un * V;
-      if (un >= nunits) break;
-      const int idx = e + (e / M) * L::V;
-      if (VEC && e + V <= nx) {
-        *reinterpret_cast<Vt *>(dst + e) = *reinterpret_cast<const Vt *>(buf + idx);
+      if constexpr (VEC) {
+        Vt x;
+        if (zero) {
+#pragma unroll
+          for (int i = 0; i < S::VN; ++i) reinterpret_cast<R *>(&x)[i] = R(0);
+        } else {
+          x = *reinterpret_cast<const Vt *>(ob + S::idx(e));
+        }
+        *reinterpret_cast<Vt *>(dst + e) = x;
       } else {
-        for (int i = 0; i < V && e + i < nx; ++i) dst[e + i] = buf[idx + i];
+        dst[e] = zero ? R(0) : ob[S::idx(e)];
       }
     }
-    __syncwarp();  // the line buffer is free for the next line
+  };
+
+  for (long long s = s0; s < s1;) {
+    const int jt = (int)(s / nz);
+    const int kb = (int)(s - (long long)jt * nz);
+    const int ke = (int)((long long)nz < kb + (s1 - s) ? (long long)nz : kb + (s1 - s));
+    s += ke - kb;
+    __syncthreads();  // the ring is free (and the factor tables are published)
+    set_tile(jt);
+#pragma unroll
+    for (int q = 0; q < LA + 2; ++q) load_plane(kb - 1 + q, kb, ke);
+    const int j = jt * J + 2 * warp;  // this warp's lines j and j + 1
+    for (int kz = kb; kz < ke; ++kz) {
+      load_plane(kz + 1 + LA, kb, ke);
+      cp_async_wait_groups<LA>();  // planes <= kz + 1 have landed
+      __syncthreads();
+      if (j < ny) {
+        R *dst = du + (long long)kz * plane + (long long)j * nx;
+        const bool kbnd = kz == 0 || kz == nz - 1;
+        const bool z0 = kbnd || j == 0 || j == ny - 1;
+        const bool z1 = kbnd || j + 1 == ny - 1;
+        const bool has1 = j + 1 < ny;
+        if (z0 && (z1 || !has1)) {
+          store_line(dst, outb, true);
+          if (has1) store_line(dst + nx, outb, true);
+        } else {
+          // slab line w2 + 1 holds line j (line 0 of the slab is j0 - 1)
+          const int w2 = 2 * warp;
+          const R *sc = ring + ((kz - kb + 1) % NS) * SL * LB;
+          const R *sm = ring + ((kz - kb) % NS) * SL * LB;
+          const R *sp = ring + ((kz - kb + 2) % NS) * SL * LB;
+          R c0[M], c1[M], d0[M], d1[M], tmp[M];
+          lds_swz<R, M>(sc + (w2 + 1) * LB, lane, c0);
+          lds_swz<R, M>(sc + (w2 + 2) * LB, lane, c1);
+          {
+            const R lf0 = shfl_up(c0[M - 1], 1, 32), rg0 = shfl_down(c0[0], 1, 32);
+            const R lf1 = shfl_up(c1[M - 1], 1, 32), rg1 = shfl_down(c1[0], 1, 32);
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+              d0[i] = (i == 0 ? lf0 : c0[i - 1]) + (i == M - 1 ? rg0 : c0[i + 1]);
+              d1[i] = (i == 0 ? lf1 : c1[i - 1]) + (i == M - 1 ? rg1 : c1[i + 1]);
+            }
+          }
+          lds_swz<R, M>(sc + w2 * LB, lane, tmp);  // j - 1 of line j
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            d0[i] = d0[i] + tmp[i];
+            d1[i] = d1[i] + c0[i];  // j - 1 of line j + 1
+          }
+          lds_swz<R, M>(sc + (w2 + 3) * LB, lane, tmp);  // j + 1 of line j + 1
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            d0[i] = d0[i] + c1[i];  // j + 1 of line j
+            d1[i] = d1[i] + tmp[i];
+          }
+          lds_swz<R, M>(sm + (w2 + 1) * LB, lane, tmp);  // k - 1
+#pragma unroll
+          for (int i = 0; i < M; ++i) d0[i] = d0[i] + tmp[i];
+          lds_swz<R, M>(sm + (w2 + 2) * LB, lane, tmp);
+#pragma unroll
+          for (int i = 0; i < M; ++i) d1[i] = d1[i] + tmp[i];
+          lds_swz<R, M>(sp + (w2 + 1) * LB, lane, tmp);  // k + 1
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            const int row = lane * M + i;
+            const R s6 = d0[i] + tmp[i];
+            d0[i] = (row >= 1 && row <= nx - 2) ? l * (s6 - R(6) * c0[i]) : R(0);
+          }
+          lds_swz<R, M>(sp + (w2 + 2) * LB, lane, tmp);
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            const int row = lane * M + i;
+            const R s6 = d1[i] + tmp[i];
+            d1[i] = (row >= 1 && row <= nx - 2) ? l * (s6 - R(6) * c1[i]) : R(0);
+          }
+          contig_solve_d2<R, M>(f, d0, d1, lane, cl);
+          sts_swz<R, M>(outb, lane, d0);
+          sts_swz<R, M>(outb + LB, lane, d1);
+          __syncwarp();
+          store_line(dst, outb, z0);
+          if (has1) store_line(dst + nx, outb + LB, z1);
+        }
+      }
+      __syncthreads();  // every warp is done with the slab of plane kz - 1
+    }
   }
+  cp_async_wait_groups<0>();
   if (warp == 0) report_bad_pivot(__any_sync(FULL_MASK, bad), flag);
 }
 
@@ -492,15 +680,16 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
           pon += stride;
         }
       }
-      const R df = j < 2 ? d * f.r[j][t] : f.r[j][t] * (d - f.ao[j][t] * dp);
+      const Pair<R> ra = f.rao[j][t];
+      const R df = j < 2 ? d * ra.x : ra.x * (d - ra.y * dp);
       rd[j] = df;
       dp = df;
     }
     // top reduced row: one running row from row M-2 up to row 1
     R Dd = rd[M - 2];
 #pragma unroll
-    for (int j = M - 3; j >= 1; --j) Dd = rd[j] - f.cf[j][t] * Dd;
-    const R topD = f.r0[t] * (rd[0] - f.cf[0][t] * Dd);
+    for (int j = M - 3; j >= 1; --j) Dd = rd[j] - f.acf[j][t].y * Dd;
+    const R topD = f.r0[t] * (rd[0] - f.acf[0][t].y * Dd);
 
     // block-wide reduced solve: re-deal the D parts so that warp w holds the
     // 32 chunks of system w, one per lane
@@ -527,7 +716,10 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
     R x = z;
 #pragma unroll
     for (int j = M - 1; j >= 0; --j) {
-      if (j < M - 1) x = j == 0 ? y : rd[j] - f.af[j][t] * y - f.cf[j][t] * x;
+      if (j < M - 1) {
+        const Pair<R> ac = f.acf[j][t];
+        x = j == 0 ? y : rd[j] - ac.x * y - ac.y * x;
+      }
       if (act && row0 + j < N) {
         if constexpr (INC)
           p.u[o] = suf[j * BS] + x;
@@ -550,27 +742,41 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
 // ---------------------------------------------------------------------------
 // Launchers.
 
-template <typename R, int M, bool VEC>
-static cudaError_t launch_adi_x_mv(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
-                                   int ny, int nz, cudaStream_t st) {
-  constexpr int NW = 8;
-  using L = SmemLayout<R, M>;
-  const size_t smem = (sizeof(ContigTab<R, M>) + 15) / 16 * 16 + (size_t)NW * L::BUF * sizeof(R);
-  auto kern = adi_x_kernel<R, M, VEC, NW>;
+template <typename R, int M, bool VEC, int J, int LA>
+static size_t adi_x_smem() {
+  return (sizeof(ContigTab<R, M>) + 15) / 16 * 16 +
+         (size_t)((LA + 3) * (J + 2) + J) * SwzLine<R, M>::LEN * sizeof(R);
+}
+
+template <typename R, int M, bool VEC, int J, int LA>
+static cudaError_t launch_adi_x_j(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
+                                  int ny, int nz, cudaStream_t st) {
+  const size_t smem = adi_x_smem<R, M, VEC, J, LA>();
+  auto kern = adi_x_kernel<R, M, VEC, J, LA>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, J * 16, smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  const long long lines = (long long)ny * nz;
-  const long long want = (lines + NW - 1) / NW;
+  const int jtiles = (ny + J - 1) / J;
+  const long long total = (long long)jtiles * nz;
   const long long cap = (long long)sms * per_sm;
-  const long long grid = want < cap ? want : cap;
-  kern<<<(unsigned)grid, NW * 32, smem, st>>>(u, du, k, flag, nx, ny, nz);
+  const long long grid = total < cap ? total : cap;
+  kern<<<(unsigned)grid, J * 16, smem, st>>>(u, du, k, flag, nx, ny, nz, jtiles);
   return cudaGetLastError();
+}
+
+// Tile of 16 lines with slabs one plane ahead where it fits in shared
+// memory, else 8 lines.
+template <typename R, int M, bool VEC>
+static cudaError_t launch_adi_x_mv(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
+                                   int ny, int nz, cudaStream_t st) {
+  if (adi_x_smem<R, M, VEC, 16, 1>() <= 224 * 1024)
+    return launch_adi_x_j<R, M, VEC, 16, 1>(u, du, k, flag, nx, ny, nz, st);
+  return launch_adi_x_j<R, M, VEC, 8, 1>(u, du, k, flag, nx, ny, nz, st);
 }
 
 template <typename R>

@@ -246,6 +246,12 @@ template <typename R> __device__ __forceinline__ void cp_async_elem(R *smem_dst,
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
+// Closes the calling thread's current group of cp.async copies (possibly
+// empty), and waits until at most N of its groups are still in flight.
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait_groups() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // 16-byte vector types for contiguous rows.
 template <typename R> struct Vec16;
