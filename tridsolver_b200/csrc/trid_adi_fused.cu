@@ -373,6 +373,10 @@ __device__ __forceinline__ void sts_swz(R *line, int lane, const R (&v)[M]) {
 }
 
 template <typename R> constexpr int adi_w() { return 128 / (int)sizeof(R); }
+// FP64 streaming CTAs of up to 8 rows per thread run two per SM (64
+// registers a thread): the second CTA's loads and sweeps fill the barrier
+// waits of the first.
+template <typename R, int M> constexpr int adi_ctas_per_sm() { return (sizeof(R) == 8 && M <= 8) ? 2 : 1; }
 template <typename R> constexpr int adi_bs() { return kT * adi_w<R>(); }
 
 }  // namespace
@@ -575,7 +579,7 @@ __global__ void __launch_bounds__(J * 16, 1)
 // right-hand side. Inc: u is carried through the window and parked in
 // private shared-memory slots until the store.
 template <typename R, int M, int D, int PF, bool INC>
-__global__ void __launch_bounds__(adi_bs<R>(), 1)
+__global__ void __launch_bounds__(adi_bs<R>(), adi_ctas_per_sm<R, M>())
     adi_stream_kernel(const BatchArgs<R> p, const ConstCoef<R> k, long long ngx, long long ngroups) {
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
   static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
@@ -603,14 +607,42 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
   }
   __syncthreads();
 
-  // element offset of this thread's first chunk row in group g; act: an
-  // interior system (others are identity systems with zero right-hand side)
-  auto group_first = [&](long long g, bool &act) -> long long {
-    const long long gx = g % ngx;
-    const long long i1 = g / ngx;
-    const long long i0 = gx * W + s;
-    act = g < ngroups && i0 >= 1 && i0 <= p.n0 - 2 && i1 >= 1 && i1 <= n1 - 2;
-    return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
+  // Group g = gx + ngx * i1 (the launcher keeps ngx and n1 below 2^31).
+  // FP64 CTAs step a cursor (gx, i1) by the grid size without dividing, in
+  // 32-bit arithmetic; FP32 CTAs (1024 threads at the 64-register limit)
+  // divide g instead, which measured faster there (fewer live registers).
+  constexpr bool kStep = sizeof(R) == 8;
+  struct Cursor {
+    int gx, i1;
+  };
+  const int ngx32 = (int)ngx;
+  const int n132 = (int)n1;
+  auto advance = [&](Cursor c) -> Cursor {
+    if constexpr (kStep) {
+      c.gx += (int)(gridDim.x % ngx32);
+      c.i1 += (int)(gridDim.x / ngx32);
+      if (c.gx >= ngx32) {
+        c.gx -= ngx32;
+        ++c.i1;
+      }
+    }
+    return c;
+  };
+  // element offset of this thread's first chunk row in group g (cursor c);
+  // act: an interior system (others are identity systems with zero
+  // right-hand side)
+  auto group_first = [&](long long g, const Cursor &c, bool &act) -> long long {
+    if constexpr (kStep) {
+      const int i0 = c.gx * W + s;
+      act = c.i1 < n132 && i0 >= 1 && i0 <= p.n0 - 2 && c.i1 >= 1 && c.i1 <= n132 - 2;
+      return act ? i0 * p.st0 + (long long)c.i1 * p.st1 + (long long)row0 * stride : 0;
+    } else {
+      const long long gx = g % ngx;
+      const long long i1 = g / ngx;
+      const long long i0 = gx * W + s;
+      act = g < ngroups && i0 >= 1 && i0 <= p.n0 - 2 && i1 >= 1 && i1 <= n1 - 2;
+      return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
+    }
   };
 
   constexpr int NA = INC ? 2 : 1;
@@ -618,19 +650,28 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
   const int pq = (lane >> 1) % NA;
   const int pt = (tid >> 5) * (32 / W) + (lane >> 1) / NA;
   const R *pbase = pq == 0 ? p.d_in : p.u;
-  auto pf_first = [&](long long g, bool &ok) -> long long {
-    const long long gx = g % ngx;
-    const long long i1 = g / ngx;
-    const long long left = p.n0 - gx * W;
-    const long long i0 = gx * W + ((lane & 1) ? (left < W ? left : W) - 1 : 0);
-    ok = pf_lane && g < ngroups;
-    return ok ? i0 * p.st0 + i1 * p.st1 + (long long)pt * M * stride : 0;
+  auto pf_first = [&](long long g, const Cursor &c, bool &ok) -> long long {
+    if constexpr (kStep) {
+      const int left = (int)p.n0 - c.gx * W;
+      const int i0 = c.gx * W + ((lane & 1) ? (left < W ? left : W) - 1 : 0);
+      ok = pf_lane && c.i1 < n132;
+      return ok ? i0 * p.st0 + (long long)c.i1 * p.st1 + (long long)pt * M * stride : 0;
+    } else {
+      const long long gx = g % ngx;
+      const long long i1 = g / ngx;
+      const long long left = p.n0 - gx * W;
+      const long long i0 = gx * W + ((lane & 1) ? (left < W ? left : W) - 1 : 0);
+      ok = pf_lane && g < ngroups;
+      return ok ? i0 * p.st0 + i1 * p.st1 + (long long)pt * M * stride : 0;
+    }
   };
 
   R pd[D], pu[INC ? D : 1];
   long long g = blockIdx.x;
+  Cursor cur{0, 0};
+  if constexpr (kStep) cur = Cursor{(int)(blockIdx.x % ngx32), (int)(blockIdx.x / ngx32)};
   bool act;
-  long long first = group_first(g, act);
+  long long first = group_first(g, cur, act);
   long long lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
@@ -641,15 +682,16 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
   }
   bool pok = false;
   long long po = 0;
-  if constexpr (PF > 0) po = pf_first(g, pok) + (long long)PF * stride;
+  if constexpr (PF > 0) po = pf_first(g, cur, pok) + (long long)PF * stride;
 
-  for (; g < ngroups; g += gridDim.x) {
+  for (; kStep ? cur.i1 < n132 : g < ngroups; g += gridDim.x) {
+    const Cursor nxt = advance(cur);
     bool actn;
-    const long long firstn = group_first(g + gridDim.x, actn);
+    const long long firstn = group_first(g + gridDim.x, nxt, actn);
     long long ln = firstn;
     bool pokn = false;
     long long pon = 0;
-    if constexpr (PF > 0) pon = pf_first(g + gridDim.x, pokn);
+    if constexpr (PF > 0) pon = pf_first(g + gridDim.x, nxt, pokn);
 
     // forward sweep of the right-hand side
     R rd[M];
@@ -728,6 +770,7 @@ __global__ void __launch_bounds__(adi_bs<R>(), 1)
       }
       o -= stride;
     }
+    cur = nxt;
     first = firstn;
     act = actn;
     lo = ln;
@@ -799,7 +842,8 @@ template <typename R, int M, int PF, bool INC>
 static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   constexpr int W = adi_w<R>();
   constexpr int BS = adi_bs<R>();
-  constexpr int D = adi_window<R, M>();
+  // (the FP64 Inc window of 8 rows spills at two CTAs per SM)
+  constexpr int D = (INC && sizeof(R) == 8 && M == 8) ? 4 : adi_window<R, M>();
   const size_t red = ((size_t)2 * kT * (W + 1) * sizeof(R) + 15) / 16 * 16;
   const size_t smem = red + (sizeof(StreamTab<R, M>) + 15) / 16 * 16 +
                       (INC ? (size_t)M * BS * sizeof(R) : 0);
@@ -832,6 +876,7 @@ static cudaError_t launch_adi_stream_m(const BatchArgs<R> &p, const ConstCoef<R>
 template <typename R, bool INC>
 cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   if (p.N < 1 || p.N > 512 || p.n0 < 1 || p.nsys % p.n0) return cudaErrorInvalidValue;
+  if (p.n0 >= (1LL << 31) || p.nsys / p.n0 >= (1LL << 31)) return cudaErrorInvalidValue;
   if (p.nsys == 0) return cudaSuccess;
   if (p.N <= 128) return launch_adi_stream_m<R, 4, INC>(p, k, st);
   if (p.N <= 256) return launch_adi_stream_m<R, 8, INC>(p, k, st);
