@@ -8,6 +8,7 @@
 #ifndef TRIDSOLVER_B200_H__
 #define TRIDSOLVER_B200_H__
 
+#include <stddef.h>
 #include <stdint.h>
 
 #include "tridsolver.h"
@@ -91,6 +92,46 @@ EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
  * ...: rows per lane of a warp per system, or 0 for 512-row tiles) and
  * returns the number of classes, or -1. */
 EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses);
+
+/* ---- distributed solve ---------------------------------------------------
+ * Counterpart of the reference's MPI/NCCL build, which links the same four
+ * strided-batch entry points (scalar/src/cuda/trid_cuda_mpi.cu:773-817) and
+ * reads its distributed parameters from ctx->mpi_params (MpiSolverParams,
+ * scalar/include/trid_mpi_solver_params.hpp:47-181). Every system is split
+ * along solvedim over nranks ranks; each rank passes its own local block
+ * (dims[solvedim] = its row count, at least 2) and rank is its position
+ * along solvedim. The partition method with the reference's ALLGATHER
+ * strategy: each rank reduces its segment of every system to two boundary
+ * rows, the rows are all-gathered, every rank solves the reduced systems,
+ * then its local segments. The exchange is the caller's allgather callback
+ * (an NCCL all-gather over NVLink from torch.distributed, or any host code):
+ *   allgather(send, recv, bytes_per_rank, user, cuda_stream)
+ * must gather bytes_per_rank bytes of device memory at `send` from every
+ * rank into `recv` in rank order (recv holds nranks * bytes_per_rank bytes),
+ * ordered after the work enqueued on cuda_stream and before later work on
+ * it; it returns 0 on success (non-zero makes the solve return
+ * TRID_STATUS_EXECUTION_FAILED after releasing its scratch).
+ * ctx->mpi_params is used only when it points at parameters registered by
+ * tridDistInit (the pointer is compared, never dereferenced otherwise, so an
+ * uninitialised mpi_params stays harmless as in the single-GPU library).
+ * The reference's other strategies (Jacobi, PCR across ranks, latency
+ * hiding by mini-batches) solve the same reduced system; this library
+ * always gathers it whole (6 values per system and rank). */
+typedef int (*tridAllgatherFn)(const void *send, void *recv, size_t bytes_per_rank, void *user,
+                               void *cuda_stream);
+typedef struct tridDistParams {
+  int solvedim; /* the split dimension; calls along other dimensions are refused */
+  int rank;     /* position along solvedim, 0 .. nranks - 1 */
+  int nranks;
+  tridAllgatherFn allgather;
+  void *user;
+} tridDistParams;
+EXTERN_C tridStatus_t tridDistInit(tridDistParams *params, int solvedim, int rank, int nranks,
+                                   tridAllgatherFn allgather, void *user);
+EXTERN_C tridStatus_t tridDistFinalize(tridDistParams *params);
+/* Bytes one rank contributes to the exchange of a call (6 values per
+ * system), or -1 for invalid arguments. */
+EXTERN_C long long tridDistExchangeBytes(int dtype_bytes, int ndim, int solvedim, const int *dims);
 
 /* ---- ADI heat-diffusion timestep -----------------------------------------
  * No single counterpart in the reference: one timestep of its ADI

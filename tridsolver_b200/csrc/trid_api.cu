@@ -146,7 +146,9 @@ static tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, b
 template <typename R, bool INC>
 static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b, const R *c, R *d,
                                   R *u, int ndim, int solvedim, const int *dims, const int *pads) {
-  (void)ctx;  // opts are hints; the autotuned plan is used for every value
+  // opts are hints (the autotuned plan is used for every value);
+  // mpi_params selects the distributed solve only when registered
+  const bool dist = ctx && dist_registered(ctx->mpi_params);
   BatchArgs<R> p;
   bool empty = false;
   tridStatus_t st = make_batch<R>(a, b, c, d, u, INC, ndim, solvedim, dims, pads, &p, &empty);
@@ -156,6 +158,9 @@ static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b,
   const Settings &cfg = settings();
   p.flag = pivot_flag_device();
   if (cfg.blocking) pivot_flag_take();  // report only this call's pivots
+  if (dist)
+    return dist_solve<R, INC>(static_cast<const tridDistParams *>(ctx->mpi_params), p, solvedim,
+                              cfg.stream, cfg.blocking);
   const Plan plan = choose_plan<R>(p, vec_aligned<R>(p));
   cudaError_t e = launch_batch<R, INC>(p, plan, cfg.stream);
   if (e != cudaSuccess) return status_of(e);

@@ -1,0 +1,317 @@
+// Distributed solve: every system is split along the solve dimension over P
+// ranks (each rank holds rows [0, n) of its segment of every system), the
+// partition method of the reference's MPI/NCCL build
+// (scalar/src/cuda/trid_cuda_mpi.cu:609-755 with the ALLGATHER strategy,
+// :218-330; forward pass scalar/src/cuda/trid_linear_mpi.hpp:49-100):
+//
+//  1. reduce: one thread per system sweeps its segment once and leaves two
+//     rows with unit diagonals that couple the segment's first and last
+//     unknowns to the neighbouring ranks' boundary unknowns,
+//         top:    A0 x_prev + x_0     + C0 x_{n-1} = D0
+//         bottom: A1 x_0    + x_{n-1} + C1 x_next  = D1;
+//     the bottom row is the last row of the forward (Thomas) elimination;
+//     the top row needs the backward elimination of rows n-2 .. 1, a chain
+//         (A, C, D) <- (a'_j - c'_j A, -c'_j C, d'_j - c'_j D)
+//     whose result is accumulated here in forward order (as sums of the
+//     rows' a', d' weighted by running products of -c'), so nothing but
+//     these six values per system is written;
+//  2. the six values of every system are gathered from all ranks (a
+//     callback: NCCL all-gather from torch.distributed, or any host code);
+//  3. finish: one thread per system solves the 2P-row reduced system of all
+//     ranks' rows (unknowns x_0 and x_{n-1} of every rank, tridiagonal in
+//     that order; the global first a and last c are ignored, as in the
+//     reference), takes the neighbours' boundary values and moves the
+//     couplings into the right-hand side,
+//         d_0 -= a_0 x_prev,   d_{n-1} -= c_{n-1} x_next;
+//  4. the local segments are then independent systems: the ordinary batched
+//     solve (which treats a_0 and c_{n-1} as zero) finishes them, so the
+//     bulk of the work runs in the library's fastest kernels.
+// For Inc, d's two corrected rows are restored afterwards.
+//
+// HBM traffic: 4 words per element for the reduction and the local solve's
+// 5, against the reference's 11 (forward writes aa, cc, dd; backward reads
+// them again).
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <set>
+
+#include "trid_internal.h"
+
+namespace trid {
+
+namespace {
+
+// Segment reduction of system s (thread per system).
+template <typename R>
+__global__ void __launch_bounds__(128) dist_reduce_kernel(const BatchArgs<R> p, R *__restrict__ out) {
+  const long long nsys = p.nsys;
+  bool bad = false;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsys;
+       s += (long long)gridDim.x * blockDim.x) {
+    const long long base = sys_base(p, s);
+    const long long st = p.stride;
+    const int n = p.N;
+    // rows 0 and 1: scaled to a unit diagonal
+    R r = rcp(__ldg(p.b + base));
+    bad |= !finite_rcp(r);
+    const R a0 = __ldg(p.a + base) * r, c0 = __ldg(p.c + base) * r, d0 = __ldg(p.d_in + base) * r;
+    R ap, cp, dp;  // the last forward row
+    // The backward chain over rows n-2 .. 1,
+    //   A_{n-2} = a'_{n-2}, A_j = a'_j - c'_j A_{j+1}  (D likewise, C_j = -c'_j C_{j+1}),
+    // unrolled: with q_1 = 1 and q_{j+1} = -c'_j q_j,
+    //   A_1 = sum_{j=1}^{n-2} q_j a'_j,  D_1 = sum_{j=1}^{n-2} q_j d'_j,
+    //   C_1 = q_{n-2} c'_{n-2} = -q_{n-1},
+    // so row j joins the sums when the sweep moves past it.
+    R q = R(1), SA = R(0), SD = R(0);
+    {
+      const long long o = base + st;
+      r = rcp(__ldg(p.b + o));
+      bad |= !finite_rcp(r);
+      ap = __ldg(p.a + o) * r;
+      cp = __ldg(p.c + o) * r;
+      dp = __ldg(p.d_in + o) * r;
+    }
+    long long o = base + 2 * st;
+    for (int j = 2; j < n; ++j, o += st) {
+      SA += q * ap;  // row j - 1 (its forward values) joins the chain
+      SD += q * dp;
+      q = -cp * q;
+      const R a = __ldg(p.a + o), b = __ldg(p.b + o), c = __ldg(p.c + o), d = __ldg(p.d_in + o);
+      r = rcp(b - a * cp);
+      bad |= !finite_rcp(r);
+      dp = r * (d - a * dp);
+      ap = -r * a * ap;
+      cp = r * c;
+    }
+    if (n >= 3) {
+      // top row: row 0 with the chain folded in (chunk_backward's last step)
+      const R C1 = -q;
+      const R rr = rcp(R(1) - c0 * SA);
+      bad |= !finite_rcp(rr);
+      out[0 * nsys + s] = rr * a0;
+      out[1 * nsys + s] = -rr * c0 * C1;
+      out[2 * nsys + s] = rr * (d0 - c0 * SD);
+    } else {
+      // n == 2: row 0 already couples x_prev, x_0 and x_1 = x_{n-1}
+      out[0 * nsys + s] = a0;
+      out[1 * nsys + s] = c0;
+      out[2 * nsys + s] = d0;
+    }
+    out[3 * nsys + s] = ap;
+    out[4 * nsys + s] = cp;
+    out[5 * nsys + s] = dp;
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+// Reduced solve of system s over all ranks' rows and the right-hand-side
+// correction of this rank's segment. g: P blocks of 6 * nsys values (the
+// gathered outputs of dist_reduce_kernel, rank-major); row i of the reduced
+// system is rank i/2's top (i even) or bottom (i odd) row, over the unknowns
+// x_0^0, x_{n-1}^0, x_0^1, ... Only the neighbours' boundary values are
+// needed (x_{2r-1} and x_{2r+2} for rank r), so the system is eliminated
+// from both ends towards them (a twisted factorisation: top-down Thomas
+// through row 2r+1, bottom-up through row 2r) with O(1) state per thread.
+// save (Inc): the two original right-hand-side values.
+constexpr int kMaxRanks = 4096;
+
+template <typename R, bool INC>
+__global__ void __launch_bounds__(128)
+    dist_finish_kernel(const BatchArgs<R> p, const R *__restrict__ g, int P, int rank,
+                       R *__restrict__ save) {
+  const long long nsys = p.nsys;
+  const int m = 2 * P;
+  bool bad = false;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsys;
+       s += (long long)gridDim.x * blockDim.x) {
+    auto row = [&](int i, R &a, R &c, R &d) {
+      const R *blk = g + (long long)(i >> 1) * 6 * nsys + ((i & 1) ? 3 : 0) * nsys + s;
+      a = i == 0 ? R(0) : blk[0];  // the global first a and last c are ignored
+      c = i == m - 1 ? R(0) : blk[nsys];
+      d = blk[2 * nsys];
+    };
+    // top-down: x_i = d'_i - c'_i x_{i+1}
+    R cp = R(0), dp = R(0), cm1 = R(0), dm1 = R(0), cp1 = R(0), dp1 = R(0);
+    const int hi = 2 * rank + 1;
+    for (int i = 0; i <= hi; ++i) {
+      R a, c, d;
+      row(i, a, c, d);
+      const R r = rcp(R(1) - a * cp);
+      bad |= !finite_rcp(r);
+      cp = c * r;
+      dp = (d - a * dp) * r;
+      if (i == 2 * rank - 1) {
+        cm1 = cp;
+        dm1 = dp;
+      }
+      if (i == hi) {
+        cp1 = cp;
+        dp1 = dp;
+      }
+    }
+    // bottom-up: x_i = f'_i - e'_i x_{i-1}
+    R ep = R(0), fp = R(0), e0 = R(0), f0 = R(0), e2 = R(0), f2 = R(0);
+    for (int i = m - 1; i >= 2 * rank; --i) {
+      R a, c, d;
+      row(i, a, c, d);
+      const R r = rcp(R(1) - c * ep);
+      bad |= !finite_rcp(r);
+      ep = a * r;
+      fp = (d - c * fp) * r;
+      if (i == 2 * rank + 2) {
+        e2 = ep;
+        f2 = fp;
+      }
+      if (i == 2 * rank) {
+        e0 = ep;
+        f0 = fp;
+      }
+    }
+    R xprev = R(0), xnext = R(0);
+    if (rank > 0) {
+      const R r = rcp(R(1) - cm1 * e0);
+      bad |= !finite_rcp(r);
+      xprev = (dm1 - cm1 * f0) * r;
+    }
+    if (rank < P - 1) {
+      const R r = rcp(R(1) - cp1 * e2);
+      bad |= !finite_rcp(r);
+      const R x1 = (dp1 - cp1 * f2) * r;  // x_{2r+1}
+      xnext = f2 - e2 * x1;
+    }
+    const long long base = sys_base(p, s);
+    const long long last = base + (long long)(p.N - 1) * p.stride;
+    R *d = const_cast<R *>(p.d_in);
+    const R d0 = d[base];
+    if constexpr (INC) save[s] = d0;
+    if (rank > 0) d[base] = d0 - __ldg(p.a + base) * xprev;
+    const R dl = d[last];
+    if constexpr (INC) save[nsys + s] = dl;
+    if (rank < P - 1) d[last] = dl - __ldg(p.c + last) * xnext;
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) dist_restore_kernel(const BatchArgs<R> p, const R *__restrict__ save) {
+  const long long nsys = p.nsys;
+  R *d = const_cast<R *>(p.d_in);
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsys;
+       s += (long long)gridDim.x * blockDim.x) {
+    const long long base = sys_base(p, s);
+    d[base] = save[s];
+    d[base + (long long)(p.N - 1) * p.stride] = save[nsys + s];
+  }
+}
+
+std::mutex g_dist_mu;
+std::set<const void *> g_dist_registered;
+
+unsigned grid_for(long long n) {
+  long long b = (n + 127) / 128;
+  if (b > 148LL * 32) b = 148LL * 32;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+bool dist_registered(const void *params) {
+  if (!params) return false;
+  std::lock_guard<std::mutex> lk(g_dist_mu);
+  return g_dist_registered.count(params) != 0;
+}
+
+template <typename R, bool INC>
+tridStatus_t dist_solve(const tridDistParams *dp, const BatchArgs<R> &p0, int solvedim,
+                        cudaStream_t st, bool blocking) {
+  if (dp->solvedim != solvedim || dp->nranks < 1 || dp->nranks > kMaxRanks || dp->rank < 0 ||
+      dp->rank >= dp->nranks || !dp->allgather)
+    return TRID_STATUS_INVALID_VALUE;
+  if (p0.N < 2) return TRID_STATUS_INVALID_VALUE;  // every rank needs two rows
+  BatchArgs<R> p = p0;
+  const int P = dp->nranks;
+  const size_t per_rank = (size_t)6 * p.nsys * sizeof(R);
+  R *scratch = nullptr;
+  const size_t save_bytes = INC ? (size_t)2 * p.nsys * sizeof(R) : 0;
+  cudaError_t e = scratch_alloc((void **)&scratch, per_rank * (1 + P) + save_bytes, st);
+  if (e != cudaSuccess) return status_of(e);
+  R *send = scratch;
+  R *recv = scratch + 6 * p.nsys;
+  R *save = recv + (size_t)6 * p.nsys * P;
+  dist_reduce_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, send);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  e = cudaGetLastError();
+  tridStatus_t status = TRID_STATUS_SUCCESS;
+  if (e == cudaSuccess) {
+    const int rc = dp->allgather(send, recv, per_rank, dp->user, st);
+    if (rc != 0) status = TRID_STATUS_EXECUTION_FAILED;
+  }
+  if (e == cudaSuccess && status == TRID_STATUS_SUCCESS) {
+    dist_finish_kernel<R, INC><<<grid_for(p.nsys), 128, 0, st>>>(p, recv, P, dp->rank, save);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && status == TRID_STATUS_SUCCESS) {
+    const Plan plan = choose_plan<R>(p, vec_aligned<R>(p));
+    e = launch_batch<R, INC>(p, plan, st);
+  }
+  if (INC && e == cudaSuccess && status == TRID_STATUS_SUCCESS) {
+    dist_restore_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, save);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    e = cudaGetLastError();
+  }
+  const cudaError_t ef = scratch_free(scratch, st);
+  if (e == cudaSuccess) e = ef;
+  if (e != cudaSuccess) return status_of(e);
+  if (status != TRID_STATUS_SUCCESS) return status;
+  if (blocking) {
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return status_of(e);
+    if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
+template tridStatus_t dist_solve<double, false>(const tridDistParams *, const BatchArgs<double> &, int,
+                                                cudaStream_t, bool);
+template tridStatus_t dist_solve<double, true>(const tridDistParams *, const BatchArgs<double> &, int,
+                                               cudaStream_t, bool);
+template tridStatus_t dist_solve<float, false>(const tridDistParams *, const BatchArgs<float> &, int,
+                                               cudaStream_t, bool);
+template tridStatus_t dist_solve<float, true>(const tridDistParams *, const BatchArgs<float> &, int,
+                                              cudaStream_t, bool);
+
+}  // namespace trid
+
+using namespace trid;
+
+EXTERN_C tridStatus_t tridDistInit(tridDistParams *params, int solvedim, int rank, int nranks,
+                                   tridAllgatherFn allgather, void *user) {
+  if (!params || !allgather || nranks < 1 || nranks > kMaxRanks || rank < 0 || rank >= nranks ||
+      solvedim < 0 || solvedim >= MAXDIM)
+    return TRID_STATUS_INVALID_VALUE;
+  params->solvedim = solvedim;
+  params->rank = rank;
+  params->nranks = nranks;
+  params->allgather = allgather;
+  params->user = user;
+  std::lock_guard<std::mutex> lk(g_dist_mu);
+  g_dist_registered.insert(params);
+  return TRID_STATUS_SUCCESS;
+}
+
+EXTERN_C tridStatus_t tridDistFinalize(tridDistParams *params) {
+  std::lock_guard<std::mutex> lk(g_dist_mu);
+  return g_dist_registered.erase(params) ? TRID_STATUS_SUCCESS : TRID_STATUS_INVALID_VALUE;
+}
+
+EXTERN_C long long tridDistExchangeBytes(int dtype_bytes, int ndim, int solvedim, const int *dims) {
+  if ((dtype_bytes != 4 && dtype_bytes != 8) || ndim < 1 || ndim > MAXDIM || solvedim < 0 ||
+      solvedim >= ndim || !dims)
+    return -1;
+  long long nsys = 1;
+  for (int i = 0; i < ndim; ++i)
+    if (i != solvedim) nsys *= dims[i];
+  return 6 * nsys * dtype_bytes;
+}

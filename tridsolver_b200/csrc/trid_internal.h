@@ -87,6 +87,13 @@ cudaError_t launch_adi_x(const R *u, R *du, const ConstCoef<R> &k, unsigned *fla
 template <typename R, bool INC>
 cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st);
 
+// Distributed solve (trid_dist.cu): whether ctx->mpi_params was registered
+// by tridDistInit, and the solve of this rank's block.
+bool dist_registered(const void *params);
+template <typename R, bool INC>
+tridStatus_t dist_solve(const tridDistParams *dp, const BatchArgs<R> &p, int solvedim,
+                        cudaStream_t st, bool blocking);
+
 // Whether every pointer and every system start allows 16-byte vector access
 // (contiguous systems only).
 template <typename R>
