@@ -48,7 +48,7 @@ def parse_args():
     ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--only-config", default=None,
-                    choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint"],
+                    choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint", "dist"],
                     help="run just one of the other configurations and print its JSON (profiling)")
     ap.add_argument("--ragged-systems", type=int, default=200000,
                     help="systems in the ragged configuration (200000 = the benchmark)")
@@ -535,6 +535,36 @@ def config_ragged(dev, hbm, nsys=200000):
     return out
 
 
+def config_dist(dev, hbm, n=512):
+    """Per-rank device cost of the distributed solve (partition method across
+    ranks): one rank's block of n^3 FP64 with a 1-rank exchange (a device
+    copy), so the reduction, the reduced solve and the local solve are timed
+    without the network; 9 words per element (4 for the reduction, 5 for the
+    local solve) against the plain solve's 5."""
+    import torch
+    import tridsolver_b200 as tb
+    from tridsolver_b200.distributed import DistContext, device_bytes
+    stream = torch.cuda.current_stream()
+    a, b, c, d = _system((n, n, n), torch.float64, dev, 21)
+    dims = [n] * 3
+
+    def local_copy(send, recv, nbytes, nranks):
+        device_bytes(recv, nbytes, dev).copy_(device_bytes(send, nbytes, dev))
+
+    out = []
+    for axis in range(3):
+        with DistContext(axis, rank=0, nranks=1, allgather=local_copy) as dc:
+            ms_dist = _timed(lambda: dc.strided_batch(a, b, c, d, dims), 5, stream)
+        ms_plain = _timed(lambda: tb.strided_batch(a, b, c, d, axis, dims), 5, stream)
+        elems = n ** 3
+        out.append({"axis": "xyz"[axis], "ms_dist": round(ms_dist, 4), "ms_plain": round(ms_plain, 4),
+                    "dist_frac": round(9 * 8 * elems / ms_dist / 1e6 / hbm, 4),
+                    "plain_frac": round(5 * 8 * elems / ms_plain / 1e6 / hbm, 4)})
+    return {"grid": dims, "dtype": "f64", "words_per_element": {"dist": 9, "plain": 5},
+            "exchange": "1 rank, device copy (per-rank device cost without the network)",
+            "results": out}
+
+
 def config_adjoint(dev, n=256, probes=1000):
     """Adjoint along y on 256^3 FP64: time against the forward solve; gradient
     entries against central finite differences (h = 1e-6) of L = sum(w x)."""
@@ -625,6 +655,7 @@ def run_configs(dev, hbm):
                      ("adi_512x512x128_f32_1000", lambda: config_adi(dev, hbm, (128, 512, 512), 1000,
                                                                       "f32")),
                      ("adjoint", lambda: config_adjoint(dev)),
+                     ("dist_512_f64", lambda: config_dist(dev, hbm)),
                      ("adi_backprop", lambda: config_adi_backprop(dev))):
         try:
             res[name] = fn()
@@ -650,7 +681,8 @@ def main():
               "adi_f32": lambda: config_adi(dev, hbm, (128, 512, 512), 1000, "f32"),
               "precision": lambda: config_precision(dev, args.n, grid),
               "ragged": lambda: config_ragged(dev, hbm, args.ragged_systems),
-              "adjoint": lambda: config_adjoint(dev)}[args.only_config]
+              "adjoint": lambda: config_adjoint(dev),
+              "dist": lambda: config_dist(dev, hbm)}[args.only_config]
         print(json.dumps({"config": args.only_config, "result": fn()}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

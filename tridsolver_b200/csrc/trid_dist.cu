@@ -72,17 +72,45 @@ __global__ void __launch_bounds__(128) dist_reduce_kernel(const BatchArgs<R> p, 
       cp = __ldg(p.c + o) * r;
       dp = __ldg(p.d_in + o) * r;
     }
-    long long o = base + 2 * st;
-    for (int j = 2; j < n; ++j, o += st) {
-      SA += q * ap;  // row j - 1 (its forward values) joins the chain
-      SD += q * dp;
-      q = -cp * q;
-      const R a = __ldg(p.a + o), b = __ldg(p.b + o), c = __ldg(p.c + o), d = __ldg(p.d_in + o);
-      r = rcp(b - a * cp);
-      bad |= !finite_rcp(r);
-      dp = r * (d - a * dp);
-      ap = -r * a * ap;
-      cp = r * c;
+    // rows 2 .. n-1 in blocks of U, the next block's loads in flight while
+    // the current one is eliminated (the sweep itself is a dependent chain)
+    constexpr int U = 4;
+    R ca[U], cb[U], cc[U], cd[U];
+    auto load_block = [&](int j0) {
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const bool v = j0 + k < n;
+        const long long o = base + (long long)(j0 + k) * st;
+        ca[k] = v ? __ldg(p.a + o) : R(0);
+        cb[k] = v ? __ldg(p.b + o) : R(1);
+        cc[k] = v ? __ldg(p.c + o) : R(0);
+        cd[k] = v ? __ldg(p.d_in + o) : R(0);
+      }
+    };
+    load_block(2);
+    for (int j0 = 2; j0 < n; j0 += U) {
+      R xa[U], xb[U], xc[U], xd[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        xa[k] = ca[k];
+        xb[k] = cb[k];
+        xc[k] = cc[k];
+        xd[k] = cd[k];
+      }
+      if (j0 + U < n) load_block(j0 + U);
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        if (j0 + k < n) {
+          SA += q * ap;  // row j - 1 (its forward values) joins the chain
+          SD += q * dp;
+          q = -cp * q;
+          r = rcp(xb[k] - xa[k] * cp);
+          bad |= !finite_rcp(r);
+          dp = r * (xd[k] - xa[k] * dp);
+          ap = -r * xa[k] * ap;
+          cp = r * xc[k];
+        }
+      }
     }
     if (n >= 3) {
       // top row: row 0 with the chain folded in (chunk_backward's last step)
