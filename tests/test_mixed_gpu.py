@@ -1,10 +1,14 @@
-"""GPU: FP32-storage solve with FP64 refinement (tridDmtsvStridedBatchMixed).
+"""GPU: FP32-storage solve to FP64 accuracy (tridDmtsvStridedBatchMixed).
 
 The system is the FP32-stored coefficients taken exactly, so the FP64 oracle
 (oracle/trid_oracle.c, the reference's Thomas recurrence) on the promoted
 coefficients is the exact answer to match: normwise relative error <= 1e-12,
 as for the plain FP64 path, across diagonal-dominance margins from 1e-3 to 1
-(the precision configuration's range) and along x, y and z.
+(the precision configuration's range) and along x, y and z. Both strategies
+are checked: the FP32 solve with FP64 refinement (mode 1, and the automatic
+choice where the direct solve does not apply) and the direct FP64 solve of
+the FP32 values (the automatic choice for strided 64 < N <= 512, which
+reports 0 refinement passes).
 """
 
 import numpy as np
@@ -36,20 +40,36 @@ SHAPES = [([512, 4, 3], 0), ([256, 8, 2], 0), ([200, 7], 0), ([33, 3], 0), ([1],
           ([16, 512, 2], 1), ([10, 300], 1), ([24, 3, 512], 2), ([40, 5, 256], 2), ([9, 2, 7], 2)]
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["auto", "refine"])
 @pytest.mark.parametrize("margin", [1e-3, 1e-1, 1.0])
 @pytest.mark.parametrize("dims,solvedim", SHAPES)
-def test_mixed_matches_fp64_oracle(dims, solvedim, margin, oracle):
+def test_mixed_matches_fp64_oracle(dims, solvedim, margin, mode, oracle):
     a32, b32, c32, d = _problem(dims, solvedim, margin, seed=sum(dims) + solvedim)
     want = d.copy()
     oracle.strided_batch(*(v.astype(np.float64) for v in (a32, b32, c32)), want, dims, solvedim)
     ta, tb_, tc = (torch.from_numpy(v).cuda() for v in (a32, b32, c32))
     td = torch.from_numpy(d).cuda()
-    st, iters, corr = tb.tridDmtsvStridedBatchMixed(None, ta, tb_, tc, td, len(dims), solvedim,
-                                                    dims, dims, max_iters=12, tol=1e-13)
+    tb.set_mixed_mode(mode)
+    try:
+        st, iters, corr = tb.tridDmtsvStridedBatchMixed(None, ta, tb_, tc, td, len(dims), solvedim,
+                                                        dims, dims, max_iters=12, tol=1e-13)
+    finally:
+        tb.set_mixed_mode(0)
     assert st == 0
-    assert 1 <= iters <= 12
+    direct = mode == 0 and solvedim >= 1 and 64 < dims[solvedim] <= 512
+    if direct:
+        assert (iters, corr) == (0, 0.0)
+    else:
+        assert 1 <= iters <= 12
     err = normwise(td.cpu().numpy(), want)
     assert err <= 1e-12, (err, iters, corr)
+
+
+def test_mixed_mode_argument():
+    with pytest.raises(tb.TridError):
+        tb.set_mixed_mode(3)
+    tb.set_mixed_mode(2)
+    tb.set_mixed_mode(0)
 
 
 def test_mixed_unsupported_cases_are_reported():

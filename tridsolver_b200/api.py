@@ -221,6 +221,15 @@ def force_stream(mode=-1):
         raise TridError(st, "tridForceStream")
 
 
+def set_mixed_mode(mode=0):
+    """tridDmtsvStridedBatchMixed strategy for this thread: 0 automatic (the
+    direct FP64 solve of the FP32 values for strided 64 < N <= 512, FP32 with
+    FP64 refinement otherwise), 1 always refinement, 2 direct where available."""
+    st = _lib.load().tridSetMixedMode(int(mode))
+    if st != 0:
+        raise TridError(st, "tridSetMixedMode")
+
+
 def describe_plan(dtype_bytes, dims, solvedim, pads=None):
     pads = dims if pads is None else pads
     buf = ctypes.create_string_buffer(128)

@@ -366,6 +366,12 @@ EXTERN_C tridStatus_t tridForceStream(int mode) {
   return TRID_STATUS_SUCCESS;
 }
 
+EXTERN_C tridStatus_t tridSetMixedMode(int mode) {
+  if (mode < 0 || mode > 2) return TRID_STATUS_INVALID_VALUE;
+  settings().mixed_mode = mode;
+  return TRID_STATUS_SUCCESS;
+}
+
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
                               const int *pads, char *buf, int buflen) {
   std::string desc;

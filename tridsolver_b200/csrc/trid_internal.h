@@ -32,6 +32,7 @@ struct Settings {
   int force_w = 0;
   int force_tma = -1;  // -1 automatic, 0 off, 1 on where it applies
   int force_stream = -1;  // -1 automatic, 0 off, 1 on where it applies
+  int mixed_mode = 0;     // tridSetMixedMode: 0 automatic, 1 refinement, 2 promoted
 };
 Settings &settings();
 
@@ -77,6 +78,10 @@ cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOu
                                           cudaStream_t st);
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
+// The streaming kernel in FP64 arithmetic on FP32-stored a, b, c.
+template <int M>
+cudaError_t launch_strided_stream_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
+                                           cudaStream_t st);
 
 // Solves of the fused ADI timestep (trid_adi_fused.cu): the x solve with the
 // 7-point stencil of u formed on the fly (du written), 1 <= nx <= 512; the y

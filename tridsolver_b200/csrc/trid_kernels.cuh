@@ -43,6 +43,12 @@ template <typename R> struct BatchArgs {
   unsigned *flag;  // host-mapped zero-pivot word (may be null)
 };
 
+// Coefficient arrays in a storage type of their own (FP32 coefficients of an
+// FP64 solve).
+template <typename CR> struct CoefPtrs {
+  const CR *a, *b, *c;
+};
+
 // Constant coefficients of one ADI heat timestep, read on the device:
 // lambda = lam[*step] (lam[0] when step is null) and, on interior rows of
 // systems through the grid's interior,

@@ -687,6 +687,36 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
   cudaError_t e = cudaMemcpyToSymbolAsync(g_mixed_stats, &zero, sizeof(zero), 0,
                                           cudaMemcpyHostToDevice, cfg.stream);
   const int N = p.N;
+  // strided batches the streaming kernel covers: the promoted solve (FP64
+  // arithmetic on the FP32 values) unless refinement is asked for
+  const bool can_promote = p.stride != 1 && N > 64 && N <= 512;
+  const bool promoted = can_promote && cfg.mixed_mode != 1;
+  if (e == cudaSuccess && promoted) {
+    BatchArgs<double> q{};
+    q.d_in = d;
+    q.d_out = d;
+    q.N = N;
+    q.nsys = p.nsys;
+    q.n0 = p.n0;
+    q.st0 = p.st0;
+    q.st1 = p.st1;
+    q.stride = p.stride;
+    q.flag = p.flag;
+    const CoefPtrs<float> cf{a, b, c};
+    e = N <= 128   ? launch_strided_stream_promoted<4>(q, cf, cfg.stream)
+        : N <= 256 ? launch_strided_stream_promoted<8>(q, cf, cfg.stream)
+                   : launch_strided_stream_promoted<16>(q, cf, cfg.stream);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (e != cudaSuccess) return status_of(e);
+    if (cfg.blocking) {
+      e = cudaStreamSynchronize(cfg.stream);
+      if (e != cudaSuccess) return status_of(e);
+      if (iters_out) *iters_out = 0;
+      if (correction_out) *correction_out = 0.0;
+      if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+    }
+    return TRID_STATUS_SUCCESS;
+  }
   if (e == cudaSuccess) {
     auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     const bool staged = p.stride == 1 && al(a) && al(b) && al(c) && al(d) && p.st0 % 4 == 0 &&

@@ -37,6 +37,8 @@
 // once.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "trid_internal.h"
 
 namespace trid {
@@ -50,18 +52,28 @@ template <typename R> constexpr int stream_bs() { return 32 * stream_w<R>(); }
 // c[N-1] forced to zero; u too for Inc. The adjoint (ADJ) solves T^T: its
 // sub-diagonal is c one row up and its super-diagonal a one row down, and
 // the fifth value is the forward solution x (in p.u).
-template <typename R, bool FIFTH, int ADJ>
-__device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, long long o, bool valid,
-                                                int row, R &a, R &b, R &c, R &d, R &u) {
+//
+// CR: the coefficients' storage type. With CR = float and R = double (the
+// promoted solve of tridDmtsvStridedBatchMixed) a, b, c are read from cf as
+// FP32 and the solve runs in FP64 on their exact promoted values.
+template <typename R, bool FIFTH, int ADJ, typename CR>
+__device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, const CoefPtrs<CR> &cf,
+                                                long long o, bool valid, int row, R &a, R &b, R &c,
+                                                R &d, R &u) {
   if (valid) {
-    if constexpr (ADJ) {
+    if constexpr (!std::is_same<CR, R>::value) {
+      a = row == 0 ? R(0) : R(__ldg(cf.a + o));
+      c = row == p.N - 1 ? R(0) : R(__ldg(cf.c + o));
+      b = R(__ldg(cf.b + o));
+    } else if constexpr (ADJ) {
       a = row == 0 ? R(0) : __ldg(p.c + o - p.stride);
       c = row == p.N - 1 ? R(0) : __ldg(p.a + o + p.stride);
+      b = __ldg(p.b + o);
     } else {
       a = row == 0 ? R(0) : __ldg(p.a + o);
       c = row == p.N - 1 ? R(0) : __ldg(p.c + o);
+      b = __ldg(p.b + o);
     }
-    b = __ldg(p.b + o);
     d = __ldg(p.d_in + o);
     if constexpr (FIFTH) u = __ldg(p.u + o);
   } else {
@@ -77,10 +89,12 @@ __device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, long long
 
 // ADJ: 0 the forward solve, 1 the adjoint (dbar only), 2 the adjoint with
 // the products abar, bbar, cbar (the forward x is read too).
-template <typename R, int M, int D, bool SD, int PF, bool INC, int ADJ>
+template <typename R, int M, int D, bool SD, int PF, bool INC, int ADJ, typename CR = R>
 __global__ void __launch_bounds__(stream_bs<R>(), 1)
-    strided_stream_kernel(const BatchArgs<R> p, const AdjointOut<R> q, long long ngx,
-                          long long ngroups) {
+    strided_stream_kernel(const BatchArgs<R> p, const AdjointOut<R> q, const CoefPtrs<CR> cf,
+                          long long ngx, long long ngroups) {
+  static_assert(std::is_same<CR, R>::value || (ADJ == 0 && PF == 0),
+                "the promoted form has neither the adjoint nor the L2 prefetch");
   static_assert(!(INC && ADJ), "Inc or adjoint");
   constexpr bool FIFTH = INC || ADJ == 2;  // a fifth value per row: u (Inc) or x (adjoint)
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
@@ -137,8 +151,8 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
   long long lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    stream_load_row<R, FIFTH, ADJ>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j],
-                                   pd[j], pu[FIFTH ? j : 0]);
+    stream_load_row<R, FIFTH, ADJ, CR>(p, cf, lo, act && row0 + j < N, row0 + j, pa[j], pb[j],
+                                       pc[j], pd[j], pu[FIFTH ? j : 0]);
     lo += stride;
   }
   bool pok = false;
@@ -170,13 +184,13 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
       if constexpr (FIFTH) suf[j * BS] = pu[k];
       if (j + D < M) {
         const int row = row0 + j + D;
-        stream_load_row<R, FIFTH, ADJ>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k],
-                                       pu[FIFTH ? k : 0]);
+        stream_load_row<R, FIFTH, ADJ, CR>(p, cf, lo, act && row < N, row, pa[k], pb[k], pc[k],
+                                           pd[k], pu[FIFTH ? k : 0]);
         lo += stride;
       } else {
         const int row = row0 + j + D - M;
-        stream_load_row<R, FIFTH, ADJ>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k],
-                                       pu[FIFTH ? k : 0]);
+        stream_load_row<R, FIFTH, ADJ, CR>(p, cf, ln, actn && row < N, row, pa[k], pb[k], pc[k],
+                                           pd[k], pu[FIFTH ? k : 0]);
         ln += stride;
       }
       if constexpr (PF > 0) {
@@ -293,16 +307,25 @@ template <typename R, int M> constexpr int stream_prefetch() {
   return stream_window<R, M>() >= M ? 0 : sizeof(R) == 8 ? 8 : (M >= 16 ? 12 : M);
 }
 
-template <typename R, int M, bool INC, int ADJ, int PF>
-static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &q, cudaStream_t st) {
+// Window of the promoted form (FP64 solve, FP32 coefficients: 5 registers
+// a row in the window instead of 8).
+template <int M> constexpr int promoted_window() { return M <= 8 ? M : 4; }
+template <int M> constexpr bool promoted_sd() { return false; }
+
+template <typename R, int M, bool INC, int ADJ, int PF, typename CR = R>
+static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &q, cudaStream_t st,
+                                    const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
   constexpr int W = stream_w<R>();
   constexpr int BS = stream_bs<R>();
-  // the adjoint's window holds 4 rows (an 8-row one spills with the products)
-  constexpr int D = ADJ && stream_window<R, M>() > 4 ? 4 : stream_window<R, M>();
-  constexpr bool SD = stream_sd<R, M>();
+  // the adjoint's window holds 4 rows (an 8-row one spills with the
+  // products); the promoted form has its own choice
+  constexpr bool PROM = !std::is_same<CR, R>::value;
+  constexpr int D = PROM ? promoted_window<M>()
+                  : ADJ && stream_window<R, M>() > 4 ? 4 : stream_window<R, M>();
+  constexpr bool SD = PROM ? promoted_sd<M>() : stream_sd<R, M>();
   const size_t red = ((size_t)6 * 32 * (W + 1) * sizeof(R) + 15) / 16 * 16;
   const size_t smem = red + (size_t)(2 + (SD ? 1 : 0) + (INC || ADJ == 2 ? 1 : 0)) * M * BS * sizeof(R);
-  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC, ADJ>;
+  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC, ADJ, CR>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -314,7 +337,7 @@ static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &
     per_sm = 1;
   const long long cap = (long long)sms * per_sm;
   const long long grid = ngroups < cap ? ngroups : cap;
-  kern<<<(unsigned)grid, BS, smem, st>>>(p, q, ngx, ngroups);
+  kern<<<(unsigned)grid, BS, smem, st>>>(p, q, cf, ngx, ngroups);
   return cudaGetLastError();
 }
 
@@ -327,6 +350,16 @@ cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaS
   if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
     return launch_stream_pf<R, M, INC, 0, PF>(p, none, st);
   return launch_stream_pf<R, M, INC, 0, 0>(p, none, st);
+}
+
+// Promoted solve: FP64 arithmetic on FP32-stored coefficients (cf), p.a,
+// p.b, p.c unused; 64 < N <= 32 M.
+template <int M>
+cudaError_t launch_strided_stream_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
+                                           cudaStream_t st) {
+  if (p.N > 32 * M) return cudaErrorInvalidValue;
+  const AdjointOut<double> none{};
+  return launch_stream_pf<double, M, false, 0, 0, float>(p, none, st, cf);
 }
 
 // Adjoint: p.a, p.b, p.c the forward coefficients, p.d_in = w, p.d_out =
@@ -366,6 +399,12 @@ INST_STREAM(double, 16)
 INST_STREAM(float, 4)
 INST_STREAM(float, 8)
 INST_STREAM(float, 16)
+template cudaError_t launch_strided_stream_promoted<4>(const BatchArgs<double> &,
+                                                       const CoefPtrs<float> &, cudaStream_t);
+template cudaError_t launch_strided_stream_promoted<8>(const BatchArgs<double> &,
+                                                       const CoefPtrs<float> &, cudaStream_t);
+template cudaError_t launch_strided_stream_promoted<16>(const BatchArgs<double> &,
+                                                        const CoefPtrs<float> &, cudaStream_t);
 template int stream_width<double>(long long);
 template int stream_width<float>(long long);
 
