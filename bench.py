@@ -476,13 +476,19 @@ def config_adi(dev, hbm, n=(256, 256, 256), steps=100, dtype="f64", alpha=1.0):
 
 def config_precision(dev, n=512, dims=None):
     """FP32 storage + FP32 solve with on-chip FP64 refinement vs the plain FP64
-    solve, along x and z, margins log-uniform [10^lo, 1]."""
+    solve, along x and z, margins log-uniform [10^lo, 1]. For strided axes the
+    library's automatic choice is the direct FP64 solve of the FP32 values;
+    both it and the refinement (forced, so its passes are reported) are timed."""
     import torch
     import tridsolver_b200 as tb
     stream = torch.cuda.current_stream()
     dims = list(dims) if dims else [n] * 3
     shape = tuple(reversed(dims))
     out = []
+
+    def mixed(a32, b32, c32, x, axis):
+        return tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, x, 3, axis, dims, dims, 12, 1e-12)
+
     for lo in (-3, -2, -1, 0):
         a, b, c, d = _system(shape, torch.float64, dev, 7 - lo, margin_lo=lo if lo < 0 else None)
         a32, b32, c32 = a.float(), b.float(), c.float()
@@ -492,21 +498,30 @@ def config_precision(dev, n=512, dims=None):
             x64 = d.clone()
             tb.set_blocking(True)
             tb.tridDmtsvStridedBatch(None, a64, b64, c64, x64, 3, axis, dims, dims)
+            tb.set_mixed_mode(1)  # the refinement, so its passes are reported
             xm = d.clone()
-            st, iters, corr = tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, xm, 3, axis, dims,
-                                                            dims, 12, 1e-12)
+            st, iters, corr = mixed(a32, b32, c32, xm, axis)
             err = ((xm - x64).abs().max() / x64.abs().max()).item()
+            tb.set_mixed_mode(0)
+            xa = d.clone()
+            st_a, iters_a, _ = mixed(a32, b32, c32, xa, axis)
+            err_a = ((xa - x64).abs().max() / x64.abs().max()).item()
             tb.set_blocking(False)
             w = d.clone()
             t64 = _timed(lambda: tb.tridDmtsvStridedBatch(None, a64, b64, c64, w, 3, axis, dims, dims),
                          5, stream)
-            tmx = _timed(lambda: tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, w, 3, axis, dims,
-                                                               dims, 12, 1e-12), 5, stream)
+            tb.set_mixed_mode(1)
+            tref = _timed(lambda: mixed(a32, b32, c32, w, axis), 5, stream)
+            tb.set_mixed_mode(0)
+            tauto = _timed(lambda: mixed(a32, b32, c32, w, axis), 5, stream)
             out.append({"margin_min": 10.0 ** lo, "axis": "xyz"[axis], "status": st,
                         "iterations": iters, "final_rel_correction": corr,
                         "max_rel_error_vs_fp64": err, "fp64_ms": round(t64, 4),
-                        "mixed_ms": round(tmx, 4), "mixed_over_fp64_time": round(tmx / t64, 3)})
-            del x64, xm, w
+                        "refine_ms": round(tref, 4),
+                        "mixed_ms": round(tauto, 4), "mixed_over_fp64_time": round(tauto / t64, 3),
+                        "mixed_strategy": "refinement" if iters_a else "direct FP64 solve of the FP32 values",
+                        "mixed_status": st_a, "mixed_error_vs_fp64": err_a})
+            del x64, xm, xa, w
         del a32, b32, c32, a64, b64, c64, d
         torch.cuda.empty_cache()
     return out
