@@ -388,9 +388,11 @@ template <typename R> constexpr int adi_bs() { return kT * adi_w<R>(); }
 // halo) stream through a ring of LA + 3 slabs in shared memory with
 // cp.async, LA planes ahead of the one being solved, so u crosses L2 about
 // once per element instead of five times. Warp w forms the 7-point
-// right-hand sides of lines j0 + 2w and j0 + 2w + 1 of plane k from the
-// slabs of planes k - 1, k, k + 1 (in the order of adi_preproc_kernel; each
-// line is the other's j neighbour), solves both with the factored
+// right-hand sides of lines j0 + 2w and j0 + 2w + 1 of plane k (in the
+// order of adi_preproc_kernel; each line is the other's j neighbour; its
+// own planes k - 1 and k are carried in registers from the previous step,
+// so each step reads two j-neighbour lines and plane k + 1 from the slabs),
+// solves both with the factored
 // coefficients (lane t = chunk t), and stores them through its own line
 // buffers, so the global stores are coalesced. Lines in shared memory use
 // the swizzled layout of SwzLine (no padding; the lanes' 16-byte chunk reads
@@ -493,6 +495,11 @@ __global__ void __launch_bounds__(J * 16, 1)
 #pragma unroll
     for (int q = 0; q < LA + 2; ++q) load_plane(kb - 1 + q, kb, ke);
     const int j = jt * J + 2 * warp;  // this warp's lines j and j + 1
+    // planes k - 1 and k of the warp's two lines, carried from the previous
+    // step (valid while `have`): each step reads only the j-neighbour lines
+    // and plane k + 1 from the slabs
+    R pm0[M], pm1[M], pc0[M], pc1[M];
+    bool have = false;
     for (int kz = kb; kz < ke; ++kz) {
       load_plane(kz + 1 + LA, kb, ke);
       cp_async_wait_groups<LA>();  // planes <= kz + 1 have landed
@@ -506,56 +513,65 @@ __global__ void __launch_bounds__(J * 16, 1)
         if (z0 && (z1 || !has1)) {
           store_line(dst, outb, true);
           if (has1) store_line(dst + nx, outb, true);
+          have = false;
         } else {
           // slab line w2 + 1 holds line j (line 0 of the slab is j0 - 1)
           const int w2 = 2 * warp;
           const R *sc = ring + ((kz - kb + 1) % NS) * SL * LB;
-          const R *sm = ring + ((kz - kb) % NS) * SL * LB;
           const R *sp = ring + ((kz - kb + 2) % NS) * SL * LB;
-          R c0[M], c1[M], d0[M], d1[M], tmp[M];
-          lds_swz<R, M>(sc + (w2 + 1) * LB, lane, c0);
-          lds_swz<R, M>(sc + (w2 + 2) * LB, lane, c1);
+          if (!have) {
+            const R *sm = ring + ((kz - kb) % NS) * SL * LB;
+            lds_swz<R, M>(sm + (w2 + 1) * LB, lane, pm0);
+            lds_swz<R, M>(sm + (w2 + 2) * LB, lane, pm1);
+            lds_swz<R, M>(sc + (w2 + 1) * LB, lane, pc0);
+            lds_swz<R, M>(sc + (w2 + 2) * LB, lane, pc1);
+          }
+          R d0[M], d1[M], tmp[M];
           {
-            const R lf0 = shfl_up(c0[M - 1], 1, 32), rg0 = shfl_down(c0[0], 1, 32);
-            const R lf1 = shfl_up(c1[M - 1], 1, 32), rg1 = shfl_down(c1[0], 1, 32);
+            const R lf0 = shfl_up(pc0[M - 1], 1, 32), rg0 = shfl_down(pc0[0], 1, 32);
+            const R lf1 = shfl_up(pc1[M - 1], 1, 32), rg1 = shfl_down(pc1[0], 1, 32);
 #pragma unroll
             for (int i = 0; i < M; ++i) {
-              d0[i] = (i == 0 ? lf0 : c0[i - 1]) + (i == M - 1 ? rg0 : c0[i + 1]);
-              d1[i] = (i == 0 ? lf1 : c1[i - 1]) + (i == M - 1 ? rg1 : c1[i + 1]);
+              d0[i] = (i == 0 ? lf0 : pc0[i - 1]) + (i == M - 1 ? rg0 : pc0[i + 1]);
+              d1[i] = (i == 0 ? lf1 : pc1[i - 1]) + (i == M - 1 ? rg1 : pc1[i + 1]);
             }
           }
           lds_swz<R, M>(sc + w2 * LB, lane, tmp);  // j - 1 of line j
 #pragma unroll
           for (int i = 0; i < M; ++i) {
             d0[i] = d0[i] + tmp[i];
-            d1[i] = d1[i] + c0[i];  // j - 1 of line j + 1
+            d1[i] = d1[i] + pc0[i];  // j - 1 of line j + 1
           }
           lds_swz<R, M>(sc + (w2 + 3) * LB, lane, tmp);  // j + 1 of line j + 1
 #pragma unroll
           for (int i = 0; i < M; ++i) {
-            d0[i] = d0[i] + c1[i];  // j + 1 of line j
+            d0[i] = d0[i] + pc1[i];  // j + 1 of line j
             d1[i] = d1[i] + tmp[i];
+            d0[i] = d0[i] + pm0[i];  // k - 1
+            d1[i] = d1[i] + pm1[i];
           }
-          lds_swz<R, M>(sm + (w2 + 1) * LB, lane, tmp);  // k - 1
-#pragma unroll
-          for (int i = 0; i < M; ++i) d0[i] = d0[i] + tmp[i];
-          lds_swz<R, M>(sm + (w2 + 2) * LB, lane, tmp);
-#pragma unroll
-          for (int i = 0; i < M; ++i) d1[i] = d1[i] + tmp[i];
-          lds_swz<R, M>(sp + (w2 + 1) * LB, lane, tmp);  // k + 1
+          // k + 1: read into the k - 1 registers, which then carry plane k + 1
+          lds_swz<R, M>(sp + (w2 + 1) * LB, lane, pm0);
+          lds_swz<R, M>(sp + (w2 + 2) * LB, lane, pm1);
 #pragma unroll
           for (int i = 0; i < M; ++i) {
             const int row = lane * M + i;
-            const R s6 = d0[i] + tmp[i];
-            d0[i] = (row >= 1 && row <= nx - 2) ? l * (s6 - R(6) * c0[i]) : R(0);
+            const bool in = row >= 1 && row <= nx - 2;
+            const R s0 = d0[i] + pm0[i];
+            const R s1 = d1[i] + pm1[i];
+            d0[i] = in ? l * (s0 - R(6) * pc0[i]) : R(0);
+            d1[i] = in ? l * (s1 - R(6) * pc1[i]) : R(0);
           }
-          lds_swz<R, M>(sp + (w2 + 2) * LB, lane, tmp);
+          // rotate: plane k becomes k - 1, plane k + 1 (in pm) becomes k
 #pragma unroll
           for (int i = 0; i < M; ++i) {
-            const int row = lane * M + i;
-            const R s6 = d1[i] + tmp[i];
-            d1[i] = (row >= 1 && row <= nx - 2) ? l * (s6 - R(6) * c1[i]) : R(0);
+            const R t0 = pc0[i], t1 = pc1[i];
+            pc0[i] = pm0[i];
+            pc1[i] = pm1[i];
+            pm0[i] = t0;
+            pm1[i] = t1;
           }
+          have = true;
           contig_solve_d2<R, M>(f, d0, d1, lane, cl);
           sts_swz<R, M>(outb, lane, d0);
           sts_swz<R, M>(outb + LB, lane, d1);
