@@ -34,31 +34,34 @@ namespace trid {
 
 namespace {
 
-constexpr int kT = 32;      // chunks per system (one warp of reduced rows)
-constexpr int kSteps = 5;   // cyclic-reduction steps over 32 reduced rows
+constexpr int kT = 32;  // chunks per system of the x solve (one warp of reduced rows)
+// cyclic-reduction steps over T reduced rows
+constexpr int pcr_steps(int T) { return T <= 1 ? 0 : 1 + pcr_steps(T / 2); }
 
 // Two table entries read with one vector load.
 template <typename R> struct alignas(2 * sizeof(R)) Pair {
   R x, y;
 };
 
-// Coefficients of the reduced system's solve (reduced_solve) by lane = chunk.
-template <typename R> struct PcrTab {
-  Pair<R> tAC[kT], bAC[kT];  // (A, C) of the top and bottom reduced rows
-  R ri[kT];
-  Pair<R> alga[kSteps][kT];  // (alpha, gamma) before each step
-  R rs[kSteps][kT];
+// Coefficients of the reduced system's solve (reduced_solve over T lanes)
+// by lane = chunk.
+template <typename R, int T = kT> struct PcrTab {
+  static constexpr int kSteps = pcr_steps(T);
+  Pair<R> tAC[T], bAC[T];  // (A, C) of the top and bottom reduced rows
+  R ri[T];
+  Pair<R> alga[kSteps][T];  // (alpha, gamma) before each step
+  R rs[kSteps][T];
 };
 
 // The coefficient half of reduced_solve for the chunk rows of lane t:
 // top row A x_prev + x + C x_last, bottom row A x_first + x + C x_next.
 // Every lane of the warp calls this.
-template <typename R>
-__device__ void pcr_factor(PcrTab<R> &q, R tA, R tC, R bA, R bC, int t, bool &bad) {
+template <typename R, int T>
+__device__ void pcr_factor(PcrTab<R, T> &q, R tA, R tC, R bA, R bC, int t, bool &bad) {
   q.tAC[t] = Pair<R>{tA, tC};
   q.bAC[t] = Pair<R>{bA, bC};
-  R pA = shfl_up(bA, 1, kT);
-  R pC = shfl_up(bC, 1, kT);
+  R pA = shfl_up(bA, 1, T);
+  R pC = shfl_up(bC, 1, T);
   if (t == 0) {
     pA = R(0);
     pC = R(0);
@@ -73,14 +76,14 @@ __device__ void pcr_factor(PcrTab<R> &q, R tA, R tC, R bA, R bC, int t, bool &ba
   ga *= r;
   int k = 0;
 #pragma unroll
-  for (int s = 1; s < kT; s <<= 1, ++k) {
-    R al_l = shfl_up(al, s, kT), ga_l = shfl_up(ga, s, kT);
-    R al_r = shfl_down(al, s, kT), ga_r = shfl_down(ga, s, kT);
+  for (int s = 1; s < T; s <<= 1, ++k) {
+    R al_l = shfl_up(al, s, T), ga_l = shfl_up(ga, s, T);
+    R al_r = shfl_down(al, s, T), ga_r = shfl_down(ga, s, T);
     if (t < s) {
       al_l = R(0);
       ga_l = R(0);
     }
-    if (t + s >= kT) {
+    if (t + s >= T) {
       al_r = R(0);
       ga_r = R(0);
     }
@@ -99,26 +102,26 @@ __device__ void pcr_factor(PcrTab<R> &q, R tA, R tC, R bA, R bC, int t, bool &ba
 // The right-hand-side half of reduced_solve: lane t holds the D parts of
 // its chunk's top and bottom reduced rows and gets the chunk's first (y) and
 // last (z) unknowns. Every lane of the warp calls this.
-template <typename R>
-__device__ __forceinline__ void pcr_solve_d(const PcrTab<R> &q, R tD, R bD, int t, R &y, R &z) {
-  R pD = shfl_up(bD, 1, kT);
+template <typename R, int T>
+__device__ __forceinline__ void pcr_solve_d(const PcrTab<R, T> &q, R tD, R bD, int t, R &y, R &z) {
+  R pD = shfl_up(bD, 1, T);
   if (t == 0) pD = R(0);
   const Pair<R> tp = q.tAC[t];
   R de = tD - tp.x * pD - tp.y * bD;
   de *= q.ri[t];
   int k = 0;
 #pragma unroll
-  for (int s = 1; s < kT; s <<= 1, ++k) {
-    R de_l = shfl_up(de, s, kT), de_r = shfl_down(de, s, kT);
+  for (int s = 1; s < T; s <<= 1, ++k) {
+    R de_l = shfl_up(de, s, T), de_r = shfl_down(de, s, T);
     if (t < s) de_l = R(0);
-    if (t + s >= kT) de_r = R(0);
+    if (t + s >= T) de_r = R(0);
     const Pair<R> ag = q.alga[k][t];
     R d2 = de - ag.x * de_l - ag.y * de_r;
     de = d2 * q.rs[k][t];
   }
   y = de;
-  R yn = shfl_down(y, 1, kT);
-  if (t == kT - 1) yn = R(0);
+  R yn = shfl_down(y, 1, T);
+  if (t == T - 1) yn = R(0);
   const Pair<R> bp = q.bAC[t];
   z = bD - bp.x * y - bp.y * yn;
 }
@@ -197,7 +200,7 @@ __device__ void contig_factor(ContigTab<R, M> &f, R ca, R cb, int N, int t, bool
   f.rb[cl] = rb;
 #pragma unroll
   for (int i = 0; i < M; ++i) f.acB[cl][i] = Pair<R>{a[i], c[i]};
-  pcr_factor<R>(f.pcr, a[0], c[0], a[M - 1], c[M - 1], t, bad);
+  pcr_factor<R, kT>(f.pcr, a[0], c[0], a[M - 1], c[M - 1], t, bad);
 }
 
 // x solves of two lines held by a warp (lane t = chunk t of class cl), in
@@ -285,15 +288,15 @@ __device__ __forceinline__ void contig_solve_d2(const ContigTab<R, M> &f, R (&d0
 
 // ---- streaming form (strided_stream_kernel) --------------------------------
 
-template <typename R, int M> struct StreamTab {
-  Pair<R> rao[M][kT];  // (forward reciprocal pivot, unscaled sub-diagonal)
-  Pair<R> acf[M][kT];  // forward (a', c')
-  R r0[kT];            // reciprocal of the top reduced row's pivot
-  PcrTab<R> pcr;
+template <typename R, int M, int T> struct StreamTab {
+  Pair<R> rao[M][T];  // (forward reciprocal pivot, unscaled sub-diagonal)
+  Pair<R> acf[M][T];  // forward (a', c')
+  R r0[T];            // reciprocal of the top reduced row's pivot
+  PcrTab<R, T> pcr;
 };
 
-template <typename R, int M>
-__device__ void stream_factor(StreamTab<R, M> &f, R ca, R cb, int N, int t, bool &bad) {
+template <typename R, int M, int T>
+__device__ void stream_factor(StreamTab<R, M, T> &f, R ca, R cb, int N, int t, bool &bad) {
   R afv[M], cfv[M];
   R ap = R(0), cp = R(0);
 #pragma unroll
@@ -330,7 +333,7 @@ __device__ void stream_factor(StreamTab<R, M> &f, R ca, R cb, int N, int t, bool
   const R r0 = rcp(R(1) - c0 * A);
   bad |= !finite_rcp(r0);
   f.r0[t] = r0;
-  pcr_factor<R>(f.pcr, r0 * a0, -r0 * c0 * C, ap, cp, t, bad);
+  pcr_factor<R, T>(f.pcr, r0 * a0, -r0 * c0 * C, ap, cp, t, bad);
 }
 
 // A line of 32 chunk rows of M elements in shared memory without padding:
@@ -373,11 +376,13 @@ __device__ __forceinline__ void sts_swz(R *line, int lane, const R (&v)[M]) {
 }
 
 template <typename R> constexpr int adi_w() { return 128 / (int)sizeof(R); }
-// FP64 streaming CTAs of up to 8 rows per thread run two per SM (64
-// registers a thread): the second CTA's loads and sweeps fill the barrier
-// waits of the first.
-template <typename R, int M> constexpr int adi_ctas_per_sm() { return (sizeof(R) == 8 && M <= 8) ? 2 : 1; }
-template <typename R> constexpr int adi_bs() { return kT * adi_w<R>(); }
+// Streaming CTAs of 512 threads run two per SM (64 registers a thread:
+// FP64 with up to 8 rows per thread, FP32 with 16 chunks per system): the
+// second CTA's loads and sweeps fill the barrier waits of the first.
+template <typename R, int M, int T> constexpr int adi_ctas_per_sm() {
+  return (sizeof(R) == 8 && M <= 8) || (sizeof(R) == 4 && T <= 16) ? 2 : 1;
+}
+template <typename R, int T> constexpr int adi_bs() { return T * adi_w<R>(); }
 
 }  // namespace
 
@@ -594,18 +599,18 @@ __global__ void __launch_bounds__(J * 16, 1)
 // prefetch PF rows ahead for rows less than 64 KiB apart), sweeping only the
 // right-hand side. Inc: u is carried through the window and parked in
 // private shared-memory slots until the store.
-template <typename R, int M, int D, int PF, bool INC>
-__global__ void __launch_bounds__(adi_bs<R>(), adi_ctas_per_sm<R, M>())
+template <typename R, int M, int D, int PF, bool INC, int T>
+__global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
     adi_stream_kernel(const BatchArgs<R> p, const ConstCoef<R> k, long long ngx, long long ngroups) {
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
   static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
   constexpr int W = adi_w<R>();
-  constexpr int BS = W * kT;
-  constexpr int RED = (2 * kT * (W + 1) * (int)sizeof(R) + 15) / 16 * 16;
+  constexpr int BS = W * T;
+  constexpr int RED = (2 * T * (W + 1) * (int)sizeof(R) + 15) / 16 * 16;
   extern __shared__ __align__(16) unsigned char stream_smem[];
   R *red = reinterpret_cast<R *>(stream_smem);
-  StreamTab<R, M> &f = *reinterpret_cast<StreamTab<R, M> *>(stream_smem + RED);
-  R *suf = reinterpret_cast<R *>(stream_smem + RED + (sizeof(StreamTab<R, M>) + 15) / 16 * 16) +
+  StreamTab<R, M, T> &f = *reinterpret_cast<StreamTab<R, M, T> *>(stream_smem + RED);
+  R *suf = reinterpret_cast<R *>(stream_smem + RED + (sizeof(StreamTab<R, M, T>) + 15) / 16 * 16) +
            threadIdx.x;  // u of row j at [j * BS] (Inc)
   const int tid = threadIdx.x;
   const int s = tid % W;
@@ -619,7 +624,8 @@ __global__ void __launch_bounds__(adi_bs<R>(), adi_ctas_per_sm<R, M>())
   {
     R l, ca, cb;
     const_coef<R>(k, l, ca, cb);
-    if (tid < 32) stream_factor<R, M>(f, ca, cb, N, lane, bad);
+    // lanes t and t + T (T < 32) compute the same values for chunk t
+    if (tid < 32) stream_factor<R, M, T>(f, ca, cb, N, lane & (T - 1), bad);
   }
   __syncthreads();
 
@@ -749,19 +755,20 @@ __global__ void __launch_bounds__(adi_bs<R>(), adi_ctas_per_sm<R, M>())
     for (int j = M - 3; j >= 1; --j) Dd = rd[j] - f.acf[j][t].y * Dd;
     const R topD = f.r0[t] * (rd[0] - f.acf[0][t].y * Dd);
 
-    // block-wide reduced solve: re-deal the D parts so that warp w holds the
-    // 32 chunks of system w, one per lane
+    // block-wide reduced solve: re-deal the D parts so that each run of T
+    // lanes holds the T chunks of one system, one per lane
     constexpr int ld = W + 1;
-    constexpr int nslot = kT * ld;
+    constexpr int nslot = T * ld;
     __syncthreads();  // the previous group's reads of red are over
     red[0 * nslot + t * ld + s] = topD;
     red[1 * nslot + t * ld + s] = dp;
     __syncthreads();
     {
-      const int s2 = tid >> 5;
-      const int kk = lane * ld + s2;
+      const int s2 = tid / T;
+      const int t2 = tid & (T - 1);
+      const int kk = t2 * ld + s2;
       R yy, zz;
-      pcr_solve_d<R>(f.pcr, red[0 * nslot + kk], red[1 * nslot + kk], lane, yy, zz);
+      pcr_solve_d<R, T>(f.pcr, red[0 * nslot + kk], red[1 * nslot + kk], t2, yy, zz);
       red[0 * nslot + kk] = yy;  // slot kk is read and rewritten by this thread only
       red[1 * nslot + kk] = zz;
     }
@@ -854,16 +861,16 @@ cudaError_t launch_adi_x(const R *u, R *du, const ConstCoef<R> &k, unsigned *fla
 template <typename R, int M> constexpr int adi_window() { return M < 8 ? M : 8; }
 template <typename R, int M> constexpr int adi_prefetch() { return adi_window<R, M>() >= M ? 0 : 12; }
 
-template <typename R, int M, int PF, bool INC>
+template <typename R, int M, int T, int PF, bool INC>
 static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   constexpr int W = adi_w<R>();
-  constexpr int BS = adi_bs<R>();
+  constexpr int BS = adi_bs<R, T>();
   // (the FP64 Inc window of 8 rows spills at two CTAs per SM)
   constexpr int D = (INC && sizeof(R) == 8 && M == 8) ? 4 : adi_window<R, M>();
-  const size_t red = ((size_t)2 * kT * (W + 1) * sizeof(R) + 15) / 16 * 16;
-  const size_t smem = red + (sizeof(StreamTab<R, M>) + 15) / 16 * 16 +
+  const size_t red = ((size_t)2 * T * (W + 1) * sizeof(R) + 15) / 16 * 16;
+  const size_t smem = red + (sizeof(StreamTab<R, M, T>) + 15) / 16 * 16 +
                       (INC ? (size_t)M * BS * sizeof(R) : 0);
-  auto kern = adi_stream_kernel<R, M, D, PF, INC>;
+  auto kern = adi_stream_kernel<R, M, D, PF, INC, T>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -879,12 +886,12 @@ static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R
   return cudaGetLastError();
 }
 
-template <typename R, int M, bool INC>
+template <typename R, int M, int T, bool INC>
 static cudaError_t launch_adi_stream_m(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   constexpr int PF = adi_prefetch<R, M>();
   if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
-    return launch_adi_stream_pf<R, M, PF, INC>(p, k, st);
-  return launch_adi_stream_pf<R, M, 0, INC>(p, k, st);
+    return launch_adi_stream_pf<R, M, T, PF, INC>(p, k, st);
+  return launch_adi_stream_pf<R, M, T, 0, INC>(p, k, st);
 }
 
 // y or z solve of the timestep: p.d_in == p.d_out == du, p.u = u for the z
@@ -894,9 +901,17 @@ cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStre
   if (p.N < 1 || p.N > 512 || p.n0 < 1 || p.nsys % p.n0) return cudaErrorInvalidValue;
   if (p.n0 >= (1LL << 31) || p.nsys / p.n0 >= (1LL << 31)) return cudaErrorInvalidValue;
   if (p.nsys == 0) return cudaSuccess;
-  if (p.N <= 128) return launch_adi_stream_m<R, 4, INC>(p, k, st);
-  if (p.N <= 256) return launch_adi_stream_m<R, 8, INC>(p, k, st);
-  return launch_adi_stream_m<R, 16, INC>(p, k, st);
+  if constexpr (sizeof(R) == 4) {
+    // FP32 systems up to 256 rows: 16 chunks of up to 16 rows (a 512-thread
+    // CTA, two per SM; the reduced solve costs half that of 32 chunks)
+    if (p.N <= 128) return launch_adi_stream_m<R, 8, 16, INC>(p, k, st);
+    if (p.N <= 256) return launch_adi_stream_m<R, 16, 16, INC>(p, k, st);
+    return launch_adi_stream_m<R, 16, 32, INC>(p, k, st);
+  } else {
+    if (p.N <= 128) return launch_adi_stream_m<R, 4, 32, INC>(p, k, st);
+    if (p.N <= 256) return launch_adi_stream_m<R, 8, 32, INC>(p, k, st);
+    return launch_adi_stream_m<R, 16, 32, INC>(p, k, st);
+  }
 }
 
 template cudaError_t launch_adi_x<double>(const double *, double *, const ConstCoef<double> &,
