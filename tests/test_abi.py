@@ -80,9 +80,9 @@ def test_empty_problem_is_success_without_device():
     (8, [8, 512, 3], 1, "hybrid M=16 T=32 W=16 stream"),
     (4, [512, 512, 512], 2, "hybrid M=16 T=32 W=32 stream"),
     (4, [512, 512, 512], 1, "hybrid M=16 T=32 W=32 stream"),
-    (4, [256, 256, 256], 1, "hybrid M=8 T=32 W=32 stream"),
+    (4, [256, 256, 256], 1, "hybrid M=16 T=16 W=32 stream"),
     (4, [3, 100, 2], 1, "hybrid M=8 T=16 W=4"),
-    (4, [16, 100, 2], 1, "hybrid M=4 T=32 W=32 stream"),
+    (4, [16, 100, 2], 1, "hybrid M=8 T=16 W=32 stream"),
     (8, [256, 256, 256], 1, "hybrid M=8 T=32 W=16 stream"),
     (8, [64, 65], 1, "hybrid M=4 T=32 W=16 stream"),
     (8, [64, 64], 1, "hybrid M=8 T=8 W=32"),

@@ -114,9 +114,18 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         const int Ws = stream_width<R>(p.n0);
         if ((fs == 1 || (fs == -1 && !want_tma && fm_ok && 2 * p.n0 >= Ws)) && N > 64 && N <= 512) {
           int Ms = N <= Ts * m_lo ? m_lo : N <= 2 * Ts * m_lo ? 2 * m_lo : 4 * m_lo;
-          if (fm > 0 && fm_ok) Ms = fm;
+          int Tsel = Ts;
+          if (fm > 0 && fm_ok) {
+            Ms = fm;
+          } else if (sizeof(R) == 4 && !p.u && N <= 256) {
+            // FP32 systems up to 256 rows: 16 chunks of up to 16 rows, a
+            // 512-thread CTA that runs two per SM (the 32-chunk form runs
+            // 1024 threads at the 64-register limit, one per SM)
+            Tsel = 16;
+            Ms = N <= 128 ? 8 : 16;
+          }
           plan.M = Ms;
-          plan.T = Ts;
+          plan.T = Tsel;
           plan.W = Ws;
           plan.streaming = true;
           return plan;

@@ -89,8 +89,8 @@ __device__ __forceinline__ void stream_load_row(const BatchArgs<R> &p, const Coe
 
 // ADJ: 0 the forward solve, 1 the adjoint (dbar only), 2 the adjoint with
 // the products abar, bbar, cbar (the forward x is read too).
-template <typename R, int M, int D, bool SD, int PF, bool INC, int ADJ, typename CR = R>
-__global__ void __launch_bounds__(stream_bs<R>(), 1)
+template <typename R, int M, int D, bool SD, int PF, bool INC, int ADJ, typename CR = R, int TC = 32>
+__global__ void __launch_bounds__(stream_w<R>() * TC, TC <= 16 ? 2 : 1)
     strided_stream_kernel(const BatchArgs<R> p, const AdjointOut<R> q, const CoefPtrs<CR> cf,
                           long long ngx, long long ngroups) {
   static_assert(std::is_same<CR, R>::value || (ADJ == 0 && PF == 0),
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(stream_bs<R>(), 1)
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
   static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
   constexpr int W = stream_w<R>();
-  constexpr int T = 32;
+  constexpr int T = TC;
   constexpr int BS = W * T;
   constexpr int RED = (6 * T * (W + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
   extern __shared__ __align__(16) unsigned char stream_smem[];
@@ -299,7 +299,9 @@ template <typename R> int stream_width(long long n0) {
 //   FP64 M=16: D=4, prefetch 8 rows ahead: 0.99 / 0.77 (D=8 with d' in
 //              shared memory spills registers: 0.82 / 0.58);
 //   FP64 M=8:  D=8: 0.91 / 0.82 (D=4: 0.77 / 0.71);
-//   FP32 M=16: D=4, prefetch 12 rows ahead: 0.87 / 0.71 (D=8 spills).
+//   FP32 M=16: D=4, prefetch 12 rows ahead: 0.87 / 0.71 (D=8 spills);
+//   FP32 up to 256 rows: 16 chunks (two 512-thread CTAs per SM): 256^3
+//              0.71 / 0.73 against 0.63 / 0.67 with 32 chunks of 8 rows.
 // The prefetch is used only for y-like layouts (see launch_strided_stream).
 template <typename R, int M> constexpr int stream_window() { return (sizeof(R) == 8 && M == 8) ? 8 : 4; }
 template <typename R, int M> constexpr bool stream_sd() { return false; }
@@ -312,20 +314,20 @@ template <typename R, int M> constexpr int stream_prefetch() {
 template <int M> constexpr int promoted_window() { return M <= 8 ? M : 4; }
 template <int M> constexpr bool promoted_sd() { return false; }
 
-template <typename R, int M, bool INC, int ADJ, int PF, typename CR = R>
+template <typename R, int M, bool INC, int ADJ, int PF, typename CR = R, int TC = 32>
 static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &q, cudaStream_t st,
                                     const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
   constexpr int W = stream_w<R>();
-  constexpr int BS = stream_bs<R>();
+  constexpr int BS = W * TC;
   // the adjoint's window holds 4 rows (an 8-row one spills with the
   // products); the promoted form has its own choice
   constexpr bool PROM = !std::is_same<CR, R>::value;
   constexpr int D = PROM ? promoted_window<M>()
                   : ADJ && stream_window<R, M>() > 4 ? 4 : stream_window<R, M>();
   constexpr bool SD = PROM ? promoted_sd<M>() : stream_sd<R, M>();
-  const size_t red = ((size_t)6 * 32 * (W + 1) * sizeof(R) + 15) / 16 * 16;
+  const size_t red = ((size_t)6 * TC * (W + 1) * sizeof(R) + 15) / 16 * 16;
   const size_t smem = red + (size_t)(2 + (SD ? 1 : 0) + (INC || ADJ == 2 ? 1 : 0)) * M * BS * sizeof(R);
-  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC, ADJ, CR>;
+  auto kern = strided_stream_kernel<R, M, D, SD, PF, INC, ADJ, CR, TC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -343,10 +345,20 @@ static cudaError_t launch_stream_pf(const BatchArgs<R> &p, const AdjointOut<R> &
 
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st) {
-  if (plan.T != 32 || plan.W != stream_w<R>() || p.N > 32 * M) return cudaErrorInvalidValue;
+  if ((plan.T != 32 && plan.T != 16) || plan.W != stream_w<R>() || p.N > plan.T * M)
+    return cudaErrorInvalidValue;
   constexpr int PF = stream_prefetch<R, M>();
   // L2 prefetch only where the rows of a system are less than 64 KiB apart
   const AdjointOut<R> none{};
+  if (plan.T == 16) {
+    // 16 chunks: FP32 forward solves of up to 256 rows (choose_plan)
+    if constexpr (sizeof(R) == 4 && !INC && (M == 8 || M == 16)) {
+      if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
+        return launch_stream_pf<R, M, INC, 0, PF, R, 16>(p, none, st);
+      return launch_stream_pf<R, M, INC, 0, 0, R, 16>(p, none, st);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
     return launch_stream_pf<R, M, INC, 0, PF>(p, none, st);
   return launch_stream_pf<R, M, INC, 0, 0>(p, none, st);
