@@ -133,6 +133,98 @@ __global__ void __launch_bounds__(128) dist_reduce_kernel(const BatchArgs<R> p, 
   report_bad_pivot(bad, p.flag);
 }
 
+// Segment reduction for contiguous rows (solvedim 0): a warp reduces 32
+// systems, one per lane, with the sweep of dist_reduce_kernel; rows arrive
+// in blocks of RB through shared memory, loaded so that each load
+// instruction reads RB consecutive rows of 32 / RB systems (full 64-byte
+// runs) instead of one row of 32 systems a line apart each.
+template <typename R>
+__global__ void __launch_bounds__(128) dist_reduce_contig_kernel(const BatchArgs<R> p,
+                                                                 R *__restrict__ out) {
+  constexpr int RB = 8;
+  constexpr int LD = RB + 1;  // odd row pitch: conflict-free per-lane reads
+  __shared__ R tile[4][4][32 * LD];  // [warp][array][system * LD + row]
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long nsys = p.nsys;
+  const int n = p.N;
+  const R *arr[4] = {p.a, p.b, p.c, p.d_in};
+  bool bad = false;
+  for (long long g0 = ((long long)blockIdx.x * 4 + warp) * 32; g0 < nsys;
+       g0 += (long long)gridDim.x * 4 * 32) {
+    const long long s = g0 + lane;
+    R a0 = R(0), c0 = R(0), d0 = R(0), ap = R(0), cp = R(0), dp = R(0);
+    R q = R(1), SA = R(0), SD = R(0);
+    // load k of a block: row lrow of system g0 + 4k + lane / RB (32 / RB = 4
+    // systems per load); their first elements, -1 past the batch
+    const int lrow = lane % RB;
+    long long lb[RB];
+#pragma unroll
+    for (int k = 0; k < RB; ++k) {
+      const long long ss = g0 + k * (32 / RB) + lane / RB;
+      lb[k] = ss < nsys ? sys_base(p, ss) : -1;
+    }
+    for (int rb = 0; rb < n; rb += RB) {
+      __syncwarp();  // the previous block's rows are consumed
+#pragma unroll
+      for (int k = 0; k < RB; ++k) {
+        const int sl = k * (32 / RB) + lane / RB;
+        const bool v = lb[k] >= 0 && rb + lrow < n;
+        const long long o = v ? lb[k] + rb + lrow : 0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) tile[warp][a][sl * LD + lrow] = v ? __ldg(arr[a] + o) : R(1);
+      }
+      __syncwarp();
+      const int rows = n - rb < RB ? n - rb : RB;
+      for (int i = 0; i < rows; ++i) {
+        const int j = rb + i;
+        const R a = tile[warp][0][lane * LD + i], b = tile[warp][1][lane * LD + i],
+                c = tile[warp][2][lane * LD + i], d = tile[warp][3][lane * LD + i];
+        if (j < 2) {
+          const R r = rcp(b);
+          bad |= !finite_rcp(r) && s < nsys;
+          if (j == 0) {
+            a0 = a * r;
+            c0 = c * r;
+            d0 = d * r;
+          } else {
+            ap = a * r;
+            cp = c * r;
+            dp = d * r;
+          }
+        } else {
+          SA += q * ap;  // row j - 1 joins the backward chain
+          SD += q * dp;
+          q = -cp * q;
+          const R r = rcp(b - a * cp);
+          bad |= !finite_rcp(r) && s < nsys;
+          dp = r * (d - a * dp);
+          ap = -r * a * ap;
+          cp = r * c;
+        }
+      }
+    }
+    if (s < nsys) {
+      if (n >= 3) {
+        const R C1 = -q;
+        const R rr = rcp(R(1) - c0 * SA);
+        bad |= !finite_rcp(rr);
+        out[0 * nsys + s] = rr * a0;
+        out[1 * nsys + s] = -rr * c0 * C1;
+        out[2 * nsys + s] = rr * (d0 - c0 * SD);
+      } else {
+        out[0 * nsys + s] = a0;
+        out[1 * nsys + s] = c0;
+        out[2 * nsys + s] = d0;
+      }
+      out[3 * nsys + s] = ap;
+      out[4 * nsys + s] = cp;
+      out[5 * nsys + s] = dp;
+    }
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
 // Reduced solve of system s over all ranks' rows and the right-hand-side
 // correction of this rank's segment. g: P blocks of 6 * nsys values (the
 // gathered outputs of dist_reduce_kernel, rank-major); row i of the reduced
@@ -267,7 +359,13 @@ tridStatus_t dist_solve(const tridDistParams *dp, const BatchArgs<R> &p0, int so
   R *send = scratch;
   R *recv = scratch + 6 * p.nsys;
   R *save = recv + (size_t)6 * p.nsys * P;
-  dist_reduce_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, send);
+  if (p.stride == 1) {
+    long long blocks = (p.nsys + 127) / 128;
+    if (blocks > 148LL * 16) blocks = 148LL * 16;
+    dist_reduce_contig_kernel<R><<<(unsigned)(blocks < 1 ? 1 : blocks), 128, 0, st>>>(p, send);
+  } else {
+    dist_reduce_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, send);
+  }
   g_launches.fetch_add(1, std::memory_order_relaxed);
   e = cudaGetLastError();
   tridStatus_t status = TRID_STATUS_SUCCESS;
