@@ -216,17 +216,19 @@ EXTERN_C tridStatus_t tridSsolveBatchedTridInc(const TridParams *ctx, int numTri
  * error estimate over all systems in *iters_out / *correction_out (-1 when
  * not blocking). Supports N <= 512 (longer systems return
  * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED).
- * Strided batches of 64 < N <= 512 rows (solvedim >= 1) are solved instead,
- * by default, in FP64 arithmetic straight from the FP32 values (the
- * streaming kernel reading a, b, c as FP32: 28 bytes per element, no
- * refinement needed, *iters_out = 0 and *correction_out = 0; the result is
- * the FP64 solve of the promoted system bit for bit): there the
- * refinement's per-row state does not fit on chip, and the direct solve is
- * about twice as fast as the refinement (still slower than
- * tridDmtsvStridedBatch on FP64 arrays: the FP32 rows of a 16-system group
- * are 64-byte segments). tridSetMixedMode (per calling thread) chooses: 0 =
- * that automatic choice (default), 1 = always the FP32 solve with FP64
- * refinement, 2 = the direct solve wherever it is available. */
+ * By default, wherever a direct kernel exists, the system is instead solved
+ * in FP64 arithmetic straight from the FP32 values (no refinement needed,
+ * *iters_out = 0 and *correction_out = 0; the result is the FP64 solve of
+ * the promoted system bit for bit): strided batches of 64 < N <= 512 rows
+ * (the streaming kernel reading a, b, c as FP32; about twice as fast as the
+ * refinement there, whose per-row state does not fit on chip, but slower
+ * than tridDmtsvStridedBatch on FP64 arrays because the FP32 rows of a
+ * 16-system group are 64-byte segments) and 16-byte-aligned contiguous
+ * systems of 129 to 512 rows (a, b, c staged in shared memory as FP32;
+ * faster than both the refinement and the FP64 solve). Both move 28 bytes
+ * per element. tridSetMixedMode (per calling thread) chooses: 0 = that
+ * automatic choice (default), 1 = always the FP32 solve with FP64
+ * refinement, 2 = the same as 0. */
 EXTERN_C tridStatus_t tridSetMixedMode(int mode);
 EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const float *a,
                                                  const float *b, const float *c, double *d,

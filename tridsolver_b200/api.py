@@ -223,8 +223,9 @@ def force_stream(mode=-1):
 
 def set_mixed_mode(mode=0):
     """tridDmtsvStridedBatchMixed strategy for this thread: 0 automatic (the
-    direct FP64 solve of the FP32 values for strided 64 < N <= 512, FP32 with
-    FP64 refinement otherwise), 1 always refinement, 2 direct where available."""
+    direct FP64 solve of the FP32 values where a direct kernel exists:
+    strided 64 < N <= 512 and aligned contiguous 129 <= N <= 512; FP32 with
+    FP64 refinement otherwise), 1 always refinement, 2 the same as 0."""
     st = _lib.load().tridSetMixedMode(int(mode))
     if st != 0:
         raise TridError(st, "tridSetMixedMode")

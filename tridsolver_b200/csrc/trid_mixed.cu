@@ -585,6 +585,117 @@ __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
 
 // ---------------------------------------------------------------------------
 
+// ---------------------------------------------------------------------------
+// Direct FP64 solve of the promoted system for contiguous, 16-byte aligned
+// systems (the automatic choice along x): contig_smem_kernel's staging with
+// a, b, c kept as FP32 in shared memory (16-byte cp.async units of 4 values)
+// and widened on the way into registers; d and x stay FP64. 28 bytes per
+// element, no refinement, the FP64 solve of the promoted values.
+template <int M>
+__global__ void __launch_bounds__(128) contig_promoted_kernel(const MixedArgs p) {
+  using LF = SmemLayout<float, M>;
+  using LD = SmemLayout<double, M>;
+  using Vd = typename Vec16<double>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PER_WARP = 3 * LF::BUF * 4 + LD::BUF * 8;  // bytes
+  unsigned char *wbase = smem_raw + (threadIdx.x >> 5) * PER_WARP;
+  float *fbuf = reinterpret_cast<float *>(wbase);                // a, b, c
+  double *dbuf = reinterpret_cast<double *>(wbase + 3 * LF::BUF * 4);
+  const int lane = threadIdx.x & 31;
+  const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (s >= p.nsys) return;  // uniform per warp
+  const long long i1 = s / p.n0;
+  const long long base = (s - i1 * p.n0) * p.st0 + i1 * p.st1;
+  const int N = p.N;
+  const float *src[3] = {p.a + base, p.b + base, p.c + base};
+  {
+    const int nu = (N + LF::V - 1) / LF::V;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      for (int un = lane; un < nu; un += 32) {
+        const int e = un * LF::V;
+        const int left = N - e;
+        cp_async16(fbuf + k * LF::BUF + e + (e / M) * LF::V, src[k] + e,
+                   (left >= LF::V ? LF::V : left) * 4);
+      }
+    const int nd = (N + LD::V - 1) / LD::V;
+    for (int un = lane; un < nd; un += 32) {
+      const int e = un * LD::V;
+      const int left = N - e;
+      cp_async16(dbuf + e + (e / M) * LD::V, p.d + base + e, (left >= LD::V ? LD::V : left) * 8);
+    }
+  }
+  cp_async_wait_all();
+  __syncwarp();
+  const int row0 = lane * M;
+  double ra[M], rb[M], rc[M], rd[M];
+  {
+    float fa[M];
+    lds_row<float, M>(fbuf + 0 * LF::BUF + lane * LF::ROW, fa);
+#pragma unroll
+    for (int i = 0; i < M; ++i) ra[i] = fa[i];
+    lds_row<float, M>(fbuf + 1 * LF::BUF + lane * LF::ROW, fa);
+#pragma unroll
+    for (int i = 0; i < M; ++i) rb[i] = fa[i];
+    lds_row<float, M>(fbuf + 2 * LF::BUF + lane * LF::ROW, fa);
+#pragma unroll
+    for (int i = 0; i < M; ++i) rc[i] = fa[i];
+  }
+  lds_row<double, M>(dbuf + lane * LD::ROW, rd);
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int row = row0 + i;
+    if (row >= N) {
+      ra[i] = 0.0;
+      rb[i] = 1.0;
+      rc[i] = 0.0;
+      rd[i] = 0.0;
+    }
+    if (row == N - 1) rc[i] = 0.0;
+  }
+  if (lane == 0) ra[0] = 0.0;
+  bool bad = false;
+  chunk_forward<double, M>(ra, rb, rc, rd, bad);
+  chunk_backward<double, M>(ra, rc, rd, bad);
+  Row<double> top{ra[0], rc[0], rd[0]};
+  Row<double> bot{ra[M - 1], rc[M - 1], rd[M - 1]};
+  double y, z;
+  reduced_solve<double>(top, bot, lane, 32, y, z, bad);
+  chunk_substitute<double, M>(ra, rc, rd, y, z);
+  __syncwarp();  // every lane has read its d row
+  sts_row<double, M>(dbuf + lane * LD::ROW, rd);
+  __syncwarp();
+  double *dst = p.d + base;
+  const int nd = (N + LD::V - 1) / LD::V;
+  for (int un = lane; un < nd; un += 32) {
+    const int e = un * LD::V;
+    const int idx = e + (e / M) * LD::V;
+    const Vd x = *reinterpret_cast<const Vd *>(dbuf + idx);
+    if (e + LD::V <= N) {
+      *reinterpret_cast<Vd *>(dst + e) = x;
+    } else {
+      dst[e] = x.x;
+    }
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+template <int M>
+static cudaError_t launch_contig_promoted(const MixedArgs &p, cudaStream_t st) {
+  using LF = SmemLayout<float, M>;
+  using LD = SmemLayout<double, M>;
+  const int threads = 128;
+  const size_t smem = (size_t)(threads / 32) * (3 * LF::BUF * 4 + LD::BUF * 8);
+  auto kern = contig_promoted_kernel<M>;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const long long blocks = (p.nsys * 32 + threads - 1) / threads;
+  kern<<<(unsigned)blocks, threads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
 static int pow2c(long long v) {
   int q = 1;
   while (q < v) q <<= 1;
@@ -722,6 +833,20 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
     const bool staged = p.stride == 1 && al(a) && al(b) && al(c) && al(d) && p.st0 % 4 == 0 &&
                         p.st1 % 4 == 0 && N > 128;
     if (N > 512) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
+    if (staged && cfg.mixed_mode != 1) {
+      // direct FP64 solve of the promoted values
+      e = N <= 256 ? launch_contig_promoted<8>(p, cfg.stream) : launch_contig_promoted<16>(p, cfg.stream);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      if (e != cudaSuccess) return status_of(e);
+      if (cfg.blocking) {
+        e = cudaStreamSynchronize(cfg.stream);
+        if (e != cudaSuccess) return status_of(e);
+        if (iters_out) *iters_out = 0;
+        if (correction_out) *correction_out = 0.0;
+        if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+      }
+      return TRID_STATUS_SUCCESS;
+    }
     if (staged) {
       e = N <= 256 ? launch_mixed_contig<8>(p, cfg.stream) : launch_mixed_contig<16>(p, cfg.stream);
     } else {
