@@ -144,7 +144,14 @@ EXTERN_C long long tridDistExchangeBytes(int dtype_bytes, int ndim, int solvedim
  *   du <- x solve; du <- y solve; u += z solve.
  * lambda = lam[*step] read on the device (lam[0] when step is NULL), and
  * *step += 1 at the end, so one captured CUDA graph of a timestep replays a
- * sequence of per-step lambdas. a, b, c, du are caller scratch of nx*ny*nz. */
+ * sequence of per-step lambdas. du is caller scratch of nx*ny*nz, and so are
+ * a, b, c when given (the reference application's coefficient arrays: a
+ * preprocessing kernel and three array solves, 21 words of memory traffic
+ * per point). With a, b, c all NULL the coefficients stay three scalars:
+ * each kernel factors the shared interior matrix once and sweeps only
+ * right-hand sides, and the 7-point stencil is formed inside the x solve
+ * (three kernels, 7 words per point; grids with an edge above 512 use the
+ * array form on library scratch instead). */
 EXTERN_C tridStatus_t tridDADIStep(double *u, double *du, double *a, double *b, double *c,
                                    const double *lam, int *step, double alpha, int nx, int ny,
                                    int nz);

@@ -93,46 +93,28 @@ static cudaError_t adi_fused(R *u, R *du, const ConstCoef<R> &k, unsigned *flag,
   return e;
 }
 
+// The array form: preprocessing kernel (RHS and one shared coefficient set)
+// and three array solves; a, b, c NULL takes them from the library's pool
+// (the fused form's fallback for systems longer than 512 rows).
 template <typename R>
-static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *step, R alpha,
-                             int nx, int ny, int nz) {
-  const bool arrays = a || b || c;
-  if (!u || !du || !lam || nx < 1 || ny < 1 || nz < 1 || (arrays && (!a || !b || !c)))
-    return TRID_STATUS_INVALID_VALUE;
-  int dev = 0, major = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
-    cudaGetLastError();
-    return TRID_STATUS_NOT_INITIALIZED;
-  }
-  if (major != 10) return TRID_STATUS_ARCH_MISMATCH;
-  const Settings &cfg = settings();
-  cudaStream_t st = cfg.stream;
-  unsigned *flag = pivot_flag_device();
-  if (cfg.blocking) pivot_flag_take();
+static cudaError_t adi_arrays(R *u, R *du, R *a, R *b, R *c, const R *lam, int *step, R alpha,
+                              unsigned *flag, int nx, int ny, int nz, cudaStream_t st) {
   const long long n = (long long)nx * ny * nz;
-  cudaError_t e = cudaSuccess;
   R *scratch = nullptr;
-  if (!arrays && nx <= 512 && ny <= 512 && nz <= 512) {
-    e = adi_fused<R>(u, du, ConstCoef<R>{lam, step, alpha}, flag, nx, ny, nz, st);
-    goto advance;
-  }
-  if (!arrays) {
-    // longer systems: the array path on pool scratch
-    e = scratch_alloc((void **)&scratch, (size_t)3 * n * sizeof(R), st);
-    if (e != cudaSuccess) return status_of(e);
+  if (!a) {
+    const cudaError_t e = scratch_alloc((void **)&scratch, (size_t)3 * n * sizeof(R), st);
+    if (e != cudaSuccess) return e;
     a = scratch;
     b = scratch + n;
     c = scratch + 2 * n;
   }
-  {
   const int threads = 256;
   long long blocks = (n + threads - 1) / threads;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   adi_preproc_kernel<R><<<(unsigned)blocks, threads, 0, st>>>(u, du, a, b, c, lam, step, alpha, nx, ny,
                                                             nz);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
   const long long dims[3] = {nx, ny, nz};
   for (int sd = 0; sd < 3 && e == cudaSuccess; ++sd) {
     BatchArgs<R> p{};
@@ -166,12 +148,35 @@ static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *s
     const Plan plan = choose_plan<R>(p, vec_aligned<R>(p), false);
     e = sd == 2 ? launch_batch<R, true>(p, plan, st) : launch_batch<R, false>(p, plan, st);
   }
-  }
   if (scratch) {
     const cudaError_t ef = scratch_free(scratch, st);
     if (e == cudaSuccess) e = ef;
   }
-advance:
+  return e;
+}
+
+template <typename R>
+static tridStatus_t adi_step(R *u, R *du, R *a, R *b, R *c, const R *lam, int *step, R alpha,
+                             int nx, int ny, int nz) {
+  const bool arrays = a || b || c;
+  if (!u || !du || !lam || nx < 1 || ny < 1 || nz < 1 || (arrays && (!a || !b || !c)))
+    return TRID_STATUS_INVALID_VALUE;
+  int dev = 0, major = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return TRID_STATUS_NOT_INITIALIZED;
+  }
+  if (major != 10) return TRID_STATUS_ARCH_MISMATCH;
+  const Settings &cfg = settings();
+  cudaStream_t st = cfg.stream;
+  unsigned *flag = pivot_flag_device();
+  if (cfg.blocking) pivot_flag_take();
+  cudaError_t e;
+  if (!arrays && nx <= 512 && ny <= 512 && nz <= 512)
+    e = adi_fused<R>(u, du, ConstCoef<R>{lam, step, alpha}, flag, nx, ny, nz, st);
+  else
+    e = adi_arrays<R>(u, du, a, b, c, lam, step, alpha, flag, nx, ny, nz, st);
   if (e == cudaSuccess && step) {
     adi_advance_kernel<<<1, 32, 0, st>>>(step);
     g_launches.fetch_add(1, std::memory_order_relaxed);
