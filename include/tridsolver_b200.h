@@ -70,10 +70,12 @@ EXTERN_C tridStatus_t tridForceStream(int mode);
  * uneven lengths: system k is rows [offsets[k], offsets[k+1]) of a, b, c, d
  * (device arrays; offsets: nsys+1 non-decreasing int64 on the device).
  * x overwrites d. Bucketed by length on the device, then solved in one
- * persistent launch: systems up to 512 (double) / 1024 (float) rows one per
- * warp with a per-length-class rows-per-lane table (pure PCR up to 32 rows,
- * the partition hybrid beyond), longer systems one per CTA (up to 16384
- * rows; a longer system makes a blocking call return
+ * persistent launch of independent warps: short systems (up to 256 rows)
+ * one per warp with a per-length-class rows-per-lane table (pure PCR up to
+ * 32 rows, the partition hybrid beyond), longer ones cut into tiles of 512
+ * rows (double) / 1024 rows (float), one warp per tile, joined by a
+ * second-level system of two rows per tile (up to 16384 rows per system; a
+ * longer system makes a blocking call return
  * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
 EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *a, const double *b,
                                            const double *c, double *d, const int64_t *offsets,
@@ -82,14 +84,14 @@ EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a
                                            const float *c, float *d, const int64_t *offsets,
                                            long long nsys);
 /* Times, per length class up to one warp's worth of rows, every
- * rows-per-lane choice of a warp per system and the staged 512-row tile
- * path, on this device (uniform synthetic batches, about a second), and
- * keeps the fastest for later ragged calls of that precision on the current
- * device. Longer systems always take 512-row tiles (up to 32 per system,
+ * rows-per-lane choice of a warp per system and the staged tile path, on
+ * this device (uniform synthetic batches, about a second), and keeps the
+ * fastest for later ragged calls of that precision on the current device.
+ * Longer systems always take tiles (512 rows double / 1024 rows float,
  * N <= 16384). */
 EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
 /* Copies the table in use (one entry per length class ceil(log2 N) = 0, 1,
- * ...: rows per lane of a warp per system, or 0 for 512-row tiles) and
+ * ...: rows per lane of a warp per system, or 0 for tiles) and
  * returns the number of classes, or -1. */
 EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses);
 

@@ -4,9 +4,10 @@ Each system is checked against the oracle's per-system Thomas solve
 (oracle_ragged_*, the reference's trid_scalar, scalar/src/cpu/
 trid_cpu.cpp:312-353): normwise <= 1e-12 (FP64) / 1e-5 (FP32), per system
 and over the batch. Lengths cover every path: empty and one-row systems,
-pure PCR (<= 32), the warp hybrid for short classes, single 512-row tiles
-and systems of 2 to 32 tiles coupled through the second-level solve (tile
-boundaries at every offset), up to the 16384-row limit, in shuffled order.
+pure PCR (<= 32), the warp hybrid for short classes, single tiles (512 rows
+FP64, 1024 rows FP32) and systems of 2 to 32 (FP32: 16) tiles coupled
+through the second-level solve (tile boundaries at every offset), up to the
+16384-row limit, in shuffled order.
 """
 
 import numpy as np
@@ -82,7 +83,7 @@ def test_autotune_then_solve(oracle):
     tb.ragged_autotune(8)
     table = tb.ragged_table(8)
     for cls, m in enumerate(table):
-        assert m == 0 or 32 * m >= 2 ** cls  # 0: 512-row tiles; else the class fits its warp
+        assert m == 0 or 32 * m >= 2 ** cls  # 0: tiles; else the class fits its warp
     lengths = np.array([5, 40, 100, 300, 500, 60, 17] * 20)
     arrs, offs = _batch(lengths, np.float64, seed=4)
     want = arrs[3].copy()
@@ -92,7 +93,8 @@ def test_autotune_then_solve(oracle):
     assert np.max(np.abs(got - want)) / np.max(np.abs(want)) <= 1e-12
 
 
-def test_too_long_system_is_reported():
-    arrs, offs = _batch(np.array([100, 16385, 7]), np.float64, seed=5)
-    st, got = _run(arrs, offs, np.float64)
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_too_long_system_is_reported(dt):
+    arrs, offs = _batch(np.array([100, 16385, 7]), dt, seed=5)
+    st, got = _run(arrs, offs, dt)
     assert st == tb.TridStatus.MATRIX_TYPE_NOT_SUPPORTED

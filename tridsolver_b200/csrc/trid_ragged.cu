@@ -5,13 +5,13 @@
 //   1. ragged_hist_kernel / ragged_order_kernel bucket the systems by length
 //      class (ceil(log2 N)), longest class first (longest-processing-time
 //      order keeps the SMs evenly loaded at the end). A system of a "tile"
-//      class is cut into K = ceil(N / 512) tiles of 512 rows and each tile
+//      class is cut into K tiles of 512 rows (FP64; 1024 rows FP32) and each tile
 //      becomes one work item; a system of a "warp" class (short systems,
 //      rows-per-lane M from the class table) is one warp item;
 //   2. ragged_kernel: persistent warps take tile items (longest systems
 //      first), then warp items, from one global counter.
 //
-// Tile item (one warp, 16 rows per lane): the warp stages the tile's rows of
+// Tile item (one warp, 16 rows per lane FP64, 32 FP32): the warp stages the tile's rows of
 // a, b, c, d in shared memory with coalesced cp.async copies, each lane runs
 // the chunk elimination on its 16 rows, and the warp's reduced solve is run
 // for three right-hand sides at once: the tile's own, and the unit
@@ -40,9 +40,13 @@
 namespace trid {
 
 constexpr int kClasses = 24;        // length classes 0..23: N <= 2^class
-constexpr int kTM = 16;             // rows per lane in tile items
-constexpr int kTileRows = 32 * kTM; // 512
-constexpr int kMaxTiles = 32;       // tiles per system: N <= 16384
+// Tile items: rows per lane (16 FP64, 32 FP32: the same bytes, registers
+// and shared memory per tile), rows per tile (512 / 1024) and tiles per
+// system (N <= 16384 either way; the second-level system has at most 64
+// rows).
+template <typename R> constexpr int tile_m() { return sizeof(R) == 8 ? 16 : 32; }
+template <typename R> constexpr int tile_rows() { return 32 * tile_m<R>(); }
+template <typename R> constexpr int max_tiles() { return 16384 / tile_rows<R>(); }
 constexpr int kRaggedThreads = 128; // 4 warps per CTA
 constexpr unsigned kWaitLimit = 1u << 22;  // polls of the ready flag (each with a short sleep)
 
@@ -96,7 +100,7 @@ __global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist, unsigned lon
     const long long n = p.off[s + 1] - p.off[s];
     const int c = length_class(n > 0 ? n : 1);
     atomicAdd(&hist[c], 1u);
-    if (p.mtab[c] == 0) atomicAdd(&tiles[c], (unsigned long long)((n + kTileRows - 1) / kTileRows));
+    if (p.mtab[c] == 0) atomicAdd(&tiles[c], (unsigned long long)((n + tile_rows<R>() - 1) / tile_rows<R>()));
   }
 }
 
@@ -113,7 +117,7 @@ __global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist,
       unsigned long long t0 = 0;
       for (int q = kClasses - 1; q > c; --q)
         if (p.mtab[q] == 0) t0 += tiles[q];
-      const long long K = (n + kTileRows - 1) / kTileRows;
+      const long long K = (n + tile_rows<R>() - 1) / tile_rows<R>();
       const long long ts = (long long)(t0 + atomicAdd(&tfill[c], (unsigned long long)K));
       if (ts + K > p.max_tiles) {  // offsets not ascending: refuse rather than overrun
         atomicExch(p.error, 3u);
@@ -258,9 +262,9 @@ __device__ __forceinline__ void reduced_solve3(const Row<R> &top, const Row<R> &
 // Shared memory of one warp's tile: a, b, c, d in padded chunk rows (as
 // contig_smem_kernel), d's rows reused for x on the way out.
 template <typename R> struct TileBuf {
-  using L = SmemLayout<R, kTM>;
+  using L = SmemLayout<R, tile_m<R>()>;
   static constexpr int ELEMS = 4 * L::BUF;
-  __device__ static __forceinline__ int slot(int e) { return (e / kTM) * L::ROW + e % kTM; }
+  __device__ static __forceinline__ int slot(int e) { return (e / tile_m<R>()) * L::ROW + e % tile_m<R>(); }
 };
 
 // Copies rows [0, nt) of the tile starting at element `base` into the warp's
@@ -271,7 +275,7 @@ template <typename R> struct TileBuf {
 template <typename R>
 __device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long base, int nt, R *buf,
                                            int lane) {
-  using L = SmemLayout<R, kTM>;
+  using L = SmemLayout<R, tile_m<R>()>;
   constexpr int V = 16 / (int)sizeof(R);
   int e0 = 0;
   if (p.vec16 && base % V == 0) {
@@ -288,7 +292,7 @@ __device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long bas
     e0 = nfull * V;
   }
 #pragma unroll 4
-  for (int e = e0 + lane; e < kTileRows; e += 32) {
+  for (int e = e0 + lane; e < tile_rows<R>(); e += 32) {
     const int o = TileBuf<R>::slot(e);
     if (e < nt) {
       cp_async_elem<R>(buf + 0 * L::BUF + o, p.a + base + e);
@@ -309,7 +313,7 @@ __device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long bas
 template <typename R>
 __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item, R *buf, int lane,
                                           bool &bad) {
-  using L = SmemLayout<R, kTM>;
+  using L = SmemLayout<R, tile_m<R>()>;
   const int4 meta = p.tile_meta[item];
   const int s = meta.x;
   const int j = meta.y;
@@ -317,10 +321,11 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
   const long long n = meta.w;
   const long long ts = item - j;
   const long long base0 = p.tile_base[item];
-  const long long r0 = (long long)j * kTileRows;
-  const int nt = (int)(n - r0 < kTileRows ? n - r0 : kTileRows);
+  const long long r0 = (long long)j * tile_rows<R>();
+  const int nt = (int)(n - r0 < tile_rows<R>() ? n - r0 : tile_rows<R>());
   stage_tile<R>(p, base0 + r0, nt, buf, lane);
 
+  constexpr int kTM = tile_m<R>();
   R a[kTM], b[kTM], c[kTM], d[kTM];
   lds_row<R, kTM>(buf + 0 * L::BUF + lane * L::ROW, a);
   lds_row<R, kTM>(buf + 1 * L::BUF + lane * L::ROW, b);
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs
     it = __shfl_sync(FULL_MASK, it, 0);
     if (it < ntiles) {
       const int4 meta = p.tile_meta[it];
-      if (meta.z > kMaxTiles) {  // longer than 16384 rows: reported once per system
+      if (meta.z > max_tiles<R>()) {  // longer than 16384 rows: reported once per system
         if (lane == 0 && meta.y == 0) atomicExch(p.error, 1u);
         continue;
       }
@@ -509,7 +514,7 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   if (e != cudaSuccess) return e;
   const long long elems = ends[1] - ends[0];
   if (elems < 0) return cudaErrorInvalidValue;
-  const long long max_tiles = elems / kTileRows + p.nsys + 1;
+  const long long max_tiles = elems / tile_rows<R>() + p.nsys + 1;
   // scratch: header | order (int, nsys) | done, ready (u32, nsys each) |
   // tile_meta (int4, max_tiles) | tile_base (i64) | tile_rows (6 R) | tile_fl (2 R)
   // header: hist u32[24] @0, fill u32[24] @128, tiles u64[24] @256,
