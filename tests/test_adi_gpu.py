@@ -37,7 +37,7 @@ def _field(shape, dtype, seed=0):
 
 @pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 1e-5)])
 @pytest.mark.parametrize("shape", [(16, 18, 20), (9, 33, 64), (40, 6, 7), (3, 5, 600),
-                                   (70, 3, 2)])
+                                   (70, 3, 2), (24, 300, 20), (300, 12, 16)])
 @pytest.mark.parametrize("alpha", [1.0, 0.5])
 @pytest.mark.parametrize("arrays", [False, True], ids=["fused", "arrays"])
 def test_native_step_against_oracle(shape, dtype, tol, alpha, arrays, oracle):
