@@ -809,7 +809,7 @@ __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
 // Launchers.
 
 template <typename R, int M, bool VEC, int J, int LA>
-static size_t adi_x_smem() {
+static constexpr size_t adi_x_smem() {
   return (sizeof(ContigTab<R, M>) + 15) / 16 * 16 +
          (size_t)((LA + 3) * (J + 2) + J) * SwzLine<R, M>::LEN * sizeof(R);
 }
@@ -840,9 +840,10 @@ static cudaError_t launch_adi_x_j(const R *u, R *du, const ConstCoef<R> &k, unsi
 template <typename R, int M, bool VEC>
 static cudaError_t launch_adi_x_mv(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
                                    int ny, int nz, cudaStream_t st) {
-  if (adi_x_smem<R, M, VEC, 16, 1>() <= 224 * 1024)
+  if constexpr (adi_x_smem<R, M, VEC, 16, 1>() <= 224 * 1024)
     return launch_adi_x_j<R, M, VEC, 16, 1>(u, du, k, flag, nx, ny, nz, st);
-  return launch_adi_x_j<R, M, VEC, 8, 1>(u, du, k, flag, nx, ny, nz, st);
+  else
+    return launch_adi_x_j<R, M, VEC, 8, 1>(u, du, k, flag, nx, ny, nz, st);
 }
 
 template <typename R>

@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(128)
     }
     const long long base = sys_base(p, s);
     const long long last = base + (long long)(p.N - 1) * p.stride;
-    R *d = const_cast<R *>(p.d_in);
+    R *d = p.d_out;  // the caller's d (d_in == d_out for both Inc and not)
     const R d0 = d[base];
     if constexpr (INC) save[s] = d0;
     if (rank > 0) d[base] = d0 - __ldg(p.a + base) * xprev;
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(128)
 template <typename R>
 __global__ void __launch_bounds__(128) dist_restore_kernel(const BatchArgs<R> p, const R *__restrict__ save) {
   const long long nsys = p.nsys;
-  R *d = const_cast<R *>(p.d_in);
+  R *d = p.d_out;  // the caller's d (d_in == d_out for both Inc and not)
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsys;
        s += (long long)gridDim.x * blockDim.x) {
     const long long base = sys_base(p, s);
