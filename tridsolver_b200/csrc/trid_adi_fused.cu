@@ -397,9 +397,8 @@ template <typename R, int T> constexpr int adi_bs() { return T * adi_w<R>(); }
 // order of adi_preproc_kernel; each line is the other's j neighbour; its
 // own planes k - 1 and k are carried in registers from the previous step,
 // so each step reads two j-neighbour lines and plane k + 1 from the slabs),
-// solves both with the factored
-// coefficients (lane t = chunk t), and stores them through its own line
-// buffers, so the global stores are coalesced. Lines in shared memory use
+// solves both with the factored coefficients (lane t = chunk t), and stores
+// them through its own line buffers, so the global stores are coalesced. Lines in shared memory use
 // the swizzled layout of SwzLine (no padding; the lanes' 16-byte chunk reads
 // are free of bank conflicts).
 //
@@ -594,11 +593,12 @@ __global__ void __launch_bounds__(J * 16, 1)
 
 // ---------------------------------------------------------------------------
 // y and z solves: the persistent streaming layout of strided_stream_kernel
-// (groups of W systems with W * sizeof(R) = 128 bytes, T = 32 chunks of M
-// rows, a D-row window of loads that runs on into the next group, L2
-// prefetch PF rows ahead for rows less than 64 KiB apart), sweeping only the
-// right-hand side. Inc: u is carried through the window and parked in
-// private shared-memory slots until the store.
+// (groups of W systems with W * sizeof(R) = 128 bytes, T chunks of M rows
+// (T = 32; 16 for FP32 systems up to 256 rows), a D-row window of loads
+// that runs on into the next group, L2 prefetch PF rows ahead for rows less
+// than 64 KiB apart), sweeping only the right-hand side. Inc: u is carried
+// through the window and parked in private shared-memory slots until the
+// store.
 template <typename R, int M, int D, int PF, bool INC, int T>
 __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
     adi_stream_kernel(const BatchArgs<R> p, const ConstCoef<R> k, long long ngx, long long ngroups) {
