@@ -88,6 +88,8 @@ def test_empty_problem_is_success_without_device():
     (8, [64, 64], 1, "hybrid M=8 T=8 W=32"),
     (8, [8, 8, 1024], 2, "hybrid M=8 T=128 W=4"),
     (4, [1024, 8], 0, "hybrid M=32 T=32"),
+    (4, [256, 256, 256], 0, "hybrid M=8 T=32 W=1 smem"),
+    (8, [256, 256, 256], 0, "hybrid M=8 T=32 W=1 smem"),
     (8, [100000], 0, "long"),
     (8, [5, 7], 1, "hybrid M=8 T=1"),
 ])
