@@ -11,6 +11,28 @@ from tridsolver_b200 import _lib
 from tridsolver_b200.api import TridParams, TridStatus
 
 
+@pytest.mark.parametrize("compiler,flags", [("gcc", ["-std=c99", "-x", "c"]),
+                                            ("g++", ["-std=c++11", "-x", "c++"])])
+def test_headers_compile_for_c_and_cxx_callers(compiler, flags, tmp_path):
+    """include/*.h is the drop-in boundary: a C or C++ caller includes it
+    as the reference's tridsolver.h, with the extensions beside it."""
+    import os
+    import shutil
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not installed")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = tmp_path / "caller.c"
+    src.write_text('#include "tridsolver.h"\n#include "tridsolver_b200.h"\n'
+                   "typedef tridStatus_t (*solve_fn)(const TridParams *, const double *,\n"
+                   "    const double *, const double *, double *, int, int, const int *,\n"
+                   "    const int *);\n"
+                   "int main(void) { tridDistParams p; TridParams ctx; solve_fn f =\n"
+                   "  tridDmtsvStridedBatch; (void)p; (void)ctx; (void)f; return 0; }\n")
+    r = subprocess.run([compiler, *flags, "-Wall", "-Werror", "-fsyntax-only", "-I", inc, str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_library_loads():
     lib = _lib.load()
     assert lib is not None
