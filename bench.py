@@ -77,7 +77,7 @@ def peaks():
 
 def ncu_traffic():
     """Per-launch DRAM bytes from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    path = os.path.join(ROOT, "profiles", "traffic_solve_kernels_512cubed_f64.txt")
     out = {}
     try:
         with open(path) as f:
