@@ -45,6 +45,32 @@ template <> struct Limits<float> {
 __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 
+// FP64 reciprocal by Newton-Raphson iteration for 1/x, r <- r + r (1 - x r)
+// (each step squares the relative error), from the hardware estimate of
+// PTX rcp.approx.ftz.f64. Two steps take the estimate to within one unit in
+// the last place (checked against 1/x on the GPU), in fewer instructions
+// than the correctly rounded form; the contiguous kernels, whose per-row work
+// is issue-bound, use it. A zero (or subnormal) x gives an infinite estimate
+// and a NaN result, which finite_rcp reports as a zero pivot. FP32 keeps the
+// correctly rounded form.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_nr(float x) { return __frcp_rn(x); }
+
+// rcp_nr when NR, else rcp
+template <bool NR, typename R> __device__ __forceinline__ R rcp_sel(R x) {
+  if constexpr (NR)
+    return rcp_nr(x);
+  else
+    return rcp(x);
+}
+
 // True when r is neither infinite nor NaN: a zero pivot gives an infinite
 // reciprocal, a NaN pivot a NaN one.
 template <typename R> __device__ __forceinline__ bool finite_rcp(R r) {
@@ -73,12 +99,13 @@ template <typename R> struct Row {
 // scaled to a unit diagonal and rows i >= 2 read
 //     a_i x_0 + x_i + c_i x_{i+1} = d_i
 // (x_0 the chunk's first unknown). b is consumed.
-template <typename R, int M>
+// NR: pivots inverted with rcp_nr instead of rcp.
+template <typename R, int M, bool NR = false>
 __device__ __forceinline__ void chunk_forward(R (&a)[M], const R (&b)[M], R (&c)[M],
                                               R (&d)[M], bool &bad) {
 #pragma unroll
   for (int i = 0; i < (M < 2 ? M : 2); ++i) {
-    R r = rcp(b[i]);
+    R r = rcp_sel<NR>(b[i]);
     bad |= !finite_rcp(r);
     a[i] *= r;
     c[i] *= r;
@@ -86,7 +113,7 @@ __device__ __forceinline__ void chunk_forward(R (&a)[M], const R (&b)[M], R (&c)
   }
 #pragma unroll
   for (int i = 2; i < M; ++i) {
-    R r = rcp(b[i] - a[i] * c[i - 1]);
+    R r = rcp_sel<NR>(b[i] - a[i] * c[i - 1]);
     bad |= !finite_rcp(r);
     d[i] = r * (d[i] - a[i] * d[i - 1]);
     a[i] = -r * a[i] * a[i - 1];
@@ -100,7 +127,7 @@ __device__ __forceinline__ void chunk_forward(R (&a)[M], const R (&b)[M], R (&c)
 // reduced row) and row M-1, untouched, reads
 //     a_{M-1} x_0 + x_{M-1} + c_{M-1} x_{next first} = d_{M-1}
 // (its bottom reduced row). For M == 2 both rows are already in that form.
-template <typename R, int M>
+template <typename R, int M, bool NR = false>
 __device__ __forceinline__ void chunk_backward(R (&a)[M], R (&c)[M], R (&d)[M], bool &bad) {
 #pragma unroll
   for (int i = M - 3; i >= 1; --i) {
@@ -109,7 +136,7 @@ __device__ __forceinline__ void chunk_backward(R (&a)[M], R (&c)[M], R (&d)[M], 
     c[i] = -c[i] * c[i + 1];
   }
   if (M >= 3) {
-    R r = rcp(R(1) - c[0] * a[1]);
+    R r = rcp_sel<NR>(R(1) - c[0] * a[1]);
     bad |= !finite_rcp(r);
     d[0] = r * (d[0] - c[0] * d[1]);
     a[0] = r * a[0];

@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(128) contig_smem_kernel(const BatchArgs<R> p) 
   }
   if (lane == 0) ra[0] = R(0);
   bool bad = false;
-  chunk_forward<R, M>(ra, rb, rc, rd, bad);
-  chunk_backward<R, M>(ra, rc, rd, bad);
+  chunk_forward<R, M, true>(ra, rb, rc, rd, bad);
+  chunk_backward<R, M, true>(ra, rc, rd, bad);
   Row<R> top{ra[0], rc[0], rd[0]};
   Row<R> bot{ra[M - 1], rc[M - 1], rd[M - 1]};
   R y, z;

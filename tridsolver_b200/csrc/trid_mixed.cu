@@ -655,8 +655,9 @@ __global__ void __launch_bounds__(128) contig_promoted_kernel(const MixedArgs p)
   }
   if (lane == 0) ra[0] = 0.0;
   bool bad = false;
-  chunk_forward<double, M>(ra, rb, rc, rd, bad);
-  chunk_backward<double, M>(ra, rc, rd, bad);
+  // the reciprocal of contig_smem_kernel, so the result is that kernel's
+  chunk_forward<double, M, true>(ra, rb, rc, rd, bad);
+  chunk_backward<double, M, true>(ra, rc, rd, bad);
   Row<double> top{ra[0], rc[0], rd[0]};
   Row<double> bot{ra[M - 1], rc[M - 1], rd[M - 1]};
   double y, z;
