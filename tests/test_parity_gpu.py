@@ -236,26 +236,28 @@ def test_zero_pivot_reported(oracle):
     assert st == 0
 
 
+@pytest.mark.parametrize("dt,emax", [(np.float64, 1000), (np.float32, 120)])
 @pytest.mark.parametrize("n", [256, 512])
-def test_contiguous_reciprocal_within_one_ulp(n):
-    """Contiguous FP64 systems invert their pivots by Newton-Raphson from the
-    hardware estimate. With a = c = 0 and d = 1 the solution is that
-    reciprocal itself, which must lie within one unit in the last place of
-    the correctly rounded 1/b, over pivots from 2^-1000 to 2^1000 of either
-    sign. A zero pivot on the same path is still reported."""
+def test_contiguous_reciprocal_within_one_ulp(n, dt, emax):
+    """Contiguous systems invert their pivots with the hardware reciprocal
+    estimate (FP64: refined by two Newton-Raphson steps). With a = c = 0 and
+    d = 1 the solution is that reciprocal itself, which must lie within one
+    unit in the last place of the correctly rounded 1/b, over pivots from
+    2^-emax to 2^emax of either sign. A zero pivot on the same path is still
+    reported."""
     dims = [n, 64]
-    assert "smem" in tb.describe_plan(8, dims, 0)
+    assert "smem" in tb.describe_plan(np.dtype(dt).itemsize, dims, 0)
     rng = np.random.default_rng(n)
     count = n * 64
-    b = rng.uniform(1.0, 2.0, count) * np.exp2(rng.integers(-1000, 1000, count).astype(np.float64))
-    b *= rng.choice([-1.0, 1.0], count)
-    a = np.zeros(count)
-    c = np.zeros(count)
-    d = np.ones(count)
+    b = rng.uniform(1.0, 2.0, count) * np.exp2(rng.integers(-emax, emax, count).astype(np.float64))
+    b = (b * rng.choice([-1.0, 1.0], count)).astype(dt)
+    a = np.zeros(count, dt)
+    c = np.zeros(count, dt)
+    d = np.ones(count, dt)
     st, out, _ = run_gpu(a, b, c, d, dims, 0)
     assert st == 0
-    want = 1.0 / b
-    ulps = np.abs(out - want) / np.spacing(np.abs(want))
+    want = (1.0 / b.astype(np.float64)).astype(dt)
+    ulps = np.abs(out.astype(np.float64) - want) / np.spacing(np.abs(want)).astype(np.float64)
     assert ulps.max() <= 1.0, ulps.max()
     b[n + 77] = 0.0
     st, out, _ = run_gpu(a, b, c, d, dims, 0)

@@ -51,8 +51,9 @@ __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 // the last place (checked against 1/x on the GPU), in fewer instructions
 // than the correctly rounded form; the contiguous kernels, whose per-row work
 // is issue-bound, use it. A zero (or subnormal) x gives an infinite estimate
-// and a NaN result, which finite_rcp reports as a zero pivot. FP32 keeps the
-// correctly rounded form.
+// and a NaN result, which finite_rcp reports as a zero pivot. In FP32 the
+// estimate rcp.approx.ftz.f32 is itself within one ulp and is used as it is
+// (a zero or subnormal x gives infinity).
 __device__ __forceinline__ double rcp_nr(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -61,7 +62,11 @@ __device__ __forceinline__ double rcp_nr(double x) {
   e = fma(-x, r, 1.0);
   return fma(r, e, r);
 }
-__device__ __forceinline__ float rcp_nr(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float rcp_nr(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // rcp_nr when NR, else rcp
 template <bool NR, typename R> __device__ __forceinline__ R rcp_sel(R x) {
