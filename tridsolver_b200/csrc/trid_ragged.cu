@@ -178,8 +178,8 @@ __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base
   } else {
     R a[M], b[M], c[M], d[M];
     ragged_load<R, M>(p, base, n, (long long)lane * M, a, b, c, d);
-    chunk_forward<R, M>(a, b, c, d, bad);
-    chunk_backward<R, M>(a, c, d, bad);
+    chunk_forward<R, M, true>(a, b, c, d, bad);
+    chunk_backward<R, M, true>(a, c, d, bad);
     R y, z;
     reduced_solve<R>(Row<R>{a[0], c[0], d[0]}, Row<R>{a[M - 1], c[M - 1], d[M - 1]}, lane, 32, y, z,
                      bad);
@@ -336,8 +336,8 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
 #pragma unroll
   for (int i = 0; i < kTM; ++i)
     if (row0 + i == n - 1) c[i] = R(0);
-  chunk_forward<R, kTM>(a, b, c, d, bad);
-  chunk_backward<R, kTM>(a, c, d, bad);
+  chunk_forward<R, kTM, true>(a, b, c, d, bad);
+  chunk_backward<R, kTM, true>(a, c, d, bad);
   const Row<R> top{a[0], c[0], d[0]}, bot{a[kTM - 1], c[kTM - 1], d[kTM - 1]};
   R y[3], z[3];
   reduced_solve3<R>(top, bot, lane == 0 ? -top.A : R(0), lane == 31 ? -bot.C : R(0), lane, y, z,
