@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
 
 #include "trid_internal.h"
 #include "tridsolver_b200.h"
@@ -484,8 +485,26 @@ __global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs
 
 // Rows per lane by length class: M > 0 for warp items, 0 for tile classes.
 // Built-in table, replaced per device and precision by tridRaggedAutotune.
+// g_tab_mu guards both: a call on one host thread may read the table while
+// tridRaggedAutotune on another replaces it.
 static int g_mtab[2][64][kClasses];
 static bool g_tuned[2][64];
+static std::mutex g_tab_mu;
+
+// The table in use for precision index pi on device dev, copied into mt;
+// false (mt untouched) when the device has no tuned table.
+static bool tuned_table(int pi, int dev, int *mt) {
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  if (!g_tuned[pi][dev]) return false;
+  memcpy(mt, g_mtab[pi][dev], sizeof(g_mtab[pi][dev]));
+  return true;
+}
+
+static void set_tuned_table(int pi, int dev, const int *mt) {
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  memcpy(g_mtab[pi][dev], mt, sizeof(g_mtab[pi][dev]));
+  g_tuned[pi][dev] = true;
+}
 
 // Longest class a warp per system may take (M <= 8); longer systems take tiles.
 template <typename R> static constexpr int ragged_warp_max() { return 256; }
@@ -613,10 +632,7 @@ static tridStatus_t ragged(const R *a, const R *b, const R *c, R *d, const int64
   if (dev < 0 || dev >= 64) return TRID_STATUS_INTERNAL_ERROR;
   const int pi = sizeof(R) == 8 ? 0 : 1;
   int mt[kClasses];
-  if (g_tuned[pi][dev])
-    memcpy(mt, g_mtab[pi][dev], sizeof(mt));
-  else
-    default_mtab<R>(mt);
+  if (!tuned_table(pi, dev, mt)) default_mtab<R>(mt);
   const Settings &cfg = settings();
   RaggedArgs<R> p{};
   p.a = a;
@@ -726,9 +742,7 @@ static tridStatus_t autotune(int dev) {
   cudaFree(buf);
   cudaFree(off);
   if (status == TRID_STATUS_SUCCESS) {
-    const int pi = sizeof(R) == 8 ? 0 : 1;
-    memcpy(g_mtab[pi][dev], mt, sizeof(mt));
-    g_tuned[pi][dev] = true;
+    set_tuned_table(sizeof(R) == 8 ? 0 : 1, dev, mt);
   }
   return status;
 }
@@ -774,12 +788,12 @@ EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses) 
   if (dev < 0 || dev >= 64 || (dtype_bytes != 8 && dtype_bytes != 4)) return -1;
   const int pi = dtype_bytes == 8 ? 0 : 1;
   int mt[kClasses];
-  if (g_tuned[pi][dev])
-    memcpy(mt, g_mtab[pi][dev], sizeof(mt));
-  else if (pi == 0)
-    default_mtab<double>(mt);
-  else
-    default_mtab<float>(mt);
+  if (!tuned_table(pi, dev, mt)) {
+    if (pi == 0)
+      default_mtab<double>(mt);
+    else
+      default_mtab<float>(mt);
+  }
   const int warp_max = pi == 0 ? ragged_warp_max<double>() : ragged_warp_max<float>();
   int n = 0;
   for (int cls = 0; cls < kClasses && (1 << cls) <= warp_max; ++cls) {
