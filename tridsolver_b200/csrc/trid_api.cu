@@ -54,8 +54,14 @@ unsigned *pivot_flag_device() {
 
 bool pivot_flag_take() {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || !g_flag_host) return false;
-  volatile unsigned *w = g_flag_host + dev;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+  unsigned *host = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_flag_mu);
+    host = g_flag_host;
+  }
+  if (!host) return false;
+  volatile unsigned *w = host + dev;
   unsigned v = *w;
   if (v) *w = 0u;
   return v != 0;
