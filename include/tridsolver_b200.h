@@ -33,6 +33,14 @@ EXTERN_C tridStatus_t tridGetPivotStatus(void);
 /* Number of kernels this library has launched in this process. */
 EXTERN_C unsigned long long tridGetLaunchCount(void);
 
+/* Returns the unused memory of the library's scratch pool on the current
+ * device to the driver. Long systems and ragged batches take their scratch
+ * from that pool, which otherwise keeps it between calls. Memory backing a
+ * call still in flight is kept, and later calls refill the pool as needed.
+ * Replaces nothing in the reference, whose scratch is static and never freed
+ * (scalar/src/cuda/trid_cuda.cu:185-206). */
+EXTERN_C tridStatus_t tridReleaseScratch(void);
+
 /* ---- plan selection ------------------------------------------------------
  * Kernel families, chosen per system length by the built-in table or the
  * autotuner:

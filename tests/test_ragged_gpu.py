@@ -98,3 +98,20 @@ def test_too_long_system_is_reported(dt):
     arrs, offs = _batch(np.array([100, 16385, 7]), dt, seed=5)
     st, got = _run(arrs, offs, dt)
     assert st == tb.TridStatus.MATRIX_TYPE_NOT_SUPPORTED
+
+
+def test_release_scratch_between_calls(oracle):
+    """tridReleaseScratch hands the scratch pool's unused memory back to the
+    driver; the next call refills the pool and gives the same result."""
+    lengths = np.array([40, 700, 5000, 3, 1500] * 40)
+    arrs, offs = _batch(lengths, np.float64, seed=6)
+    st, first = _run(arrs, offs, np.float64)
+    assert st == 0
+    tb.release_scratch()
+    tb.release_scratch()
+    st, second = _run(arrs, offs, np.float64)
+    assert st == 0
+    assert np.array_equal(first, second)
+    want = arrs[3].copy()
+    oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
+    assert np.max(np.abs(second - want)) / np.max(np.abs(want)) <= 1e-12

@@ -34,6 +34,7 @@ SYMBOLS = {
     "tridGetBlocking": (_I, []),
     "tridGetPivotStatus": (_I, []),
     "tridGetLaunchCount": (ctypes.c_ulonglong, []),
+    "tridReleaseScratch": (_I, []),
     "tridForcePlan": (_I, [_I, _I]),
     "tridForceSystemsPerBlock": (_I, [_I]),
     "tridForceTma": (_I, [_I]),

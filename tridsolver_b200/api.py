@@ -194,6 +194,14 @@ def launch_count():
     return int(_lib.load().tridGetLaunchCount())
 
 
+def release_scratch():
+    """Return the unused memory of the library's scratch pool on the current
+    device to the driver (tridReleaseScratch)."""
+    st = _lib.load().tridReleaseScratch()
+    if st != 0:
+        raise TridError(st, "tridReleaseScratch")
+
+
 def force_plan(family=FAMILY_AUTO, rows_per_thread=0):
     st = _lib.load().tridForcePlan(int(family), int(rows_per_thread))
     if st != 0:

@@ -337,6 +337,8 @@ EXTERN_C tridStatus_t tridGetPivotStatus(void) {
 
 EXTERN_C unsigned long long tridGetLaunchCount(void) { return g_launches.load(); }
 
+EXTERN_C tridStatus_t tridReleaseScratch(void) { return status_of(scratch_release()); }
+
 EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread) {
   Settings &s = settings();
   if (family < 0) {

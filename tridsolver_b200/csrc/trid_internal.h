@@ -41,6 +41,7 @@ extern std::atomic<unsigned long long> g_launches;
 // Stream-ordered scratch from the library's own pool (trid_pool.cu).
 cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t st);
 cudaError_t scratch_free(void *ptr, cudaStream_t st);
+cudaError_t scratch_release();
 
 // Host-mapped zero-pivot word of the current device (device pointer), or
 // nullptr if it could not be set up.

@@ -6,6 +6,7 @@
 // of 200,000 systems. The default pool of the process is left untouched.
 // While a stream is being captured into a CUDA graph the default pool is
 // used, so the allocation becomes a graph memory node as usual.
+// tridReleaseScratch trims the pool back to nothing on request.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -58,5 +59,18 @@ cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t st) {
 }
 
 cudaError_t scratch_free(void *ptr, cudaStream_t st) { return cudaFreeAsync(ptr, st); }
+
+// Hands the unused memory of the current device's library pool back to the
+// driver. Memory that backs an allocation still in use (a call in flight on
+// some stream) stays; the pool keeps serving later calls.
+cudaError_t scratch_release() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_pools[dev]) return cudaSuccess;
+  return cudaMemPoolTrimTo(g_pools[dev], 0);
+}
 
 }  // namespace trid
