@@ -93,6 +93,18 @@ def test_empty_problem_is_success_without_device():
     assert st == TridStatus.SUCCESS
 
 
+def test_release_scratch_reports_missing_device():
+    """Without a usable device the release returns an error status (raised
+    as TridError), it does not crash."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU tests cover the release")
+    st = tb.load_library().tridReleaseScratch()
+    assert st != TridStatus.SUCCESS
+    with pytest.raises(tb.TridError):
+        tb.release_scratch()
+
+
 @pytest.mark.parametrize("dtype_bytes,dims,solvedim,expect", [
     (8, [512, 512, 512], 0, "hybrid M=16 T=32 W=1 smem"),
     (8, [512, 512, 512], 2, "hybrid M=16 T=32 W=16 stream"),
