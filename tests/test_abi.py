@@ -33,6 +33,46 @@ def test_headers_compile_for_c_and_cxx_callers(compiler, flags, tmp_path):
     assert r.returncode == 0, r.stderr
 
 
+def test_c_caller_links_and_runs_without_device(tmp_path):
+    """A C program written against the reference's header links against the
+    library in its place (-ltridsolver_b200 instead of -ltridcuda) and runs:
+    argument errors and empty problems are answered before any device is
+    touched, and a real solve without a usable device returns an error
+    status instead of exiting."""
+    import os
+    import shutil
+    import torch
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not installed")
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU tests run real solves")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "tridsolver.h"\n'
+        "int main(void) {\n"
+        "  double buf[8] = {0};\n"
+        "  int dims[1] = {8}, pads[1] = {8}, empty[1] = {0};\n"
+        "  TridParams ctx = {0};\n"
+        "  tridStatus_t bad = tridDmtsvStridedBatch(&ctx, buf, buf, buf, buf, 1, 1, dims, pads);\n"
+        "  tridStatus_t none = tridDmtsvStridedBatch(&ctx, buf, buf, buf, buf, 1, 0, empty, empty);\n"
+        "  tridStatus_t real = tridDmtsvStridedBatch(&ctx, buf, buf, buf, buf, 1, 0, dims, pads);\n"
+        '  printf("%d %d %d\\n", (int)bad, (int)none, (int)real);\n'
+        "  return 0;\n}\n")
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+                        str(src), "-o", str(exe), "-L", libdir, "-ltridsolver_b200",
+                        f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    bad, none, real = (int(v) for v in r.stdout.split())
+    assert bad == TridStatus.INVALID_VALUE
+    assert none == TridStatus.SUCCESS
+    assert real not in (TridStatus.SUCCESS, TridStatus.INVALID_VALUE)
+
+
 def test_library_loads():
     lib = _lib.load()
     assert lib is not None
