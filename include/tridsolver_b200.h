@@ -41,6 +41,16 @@ EXTERN_C unsigned long long tridGetLaunchCount(void);
  * (scalar/src/cuda/trid_cuda.cu:185-206). */
 EXTERN_C tridStatus_t tridReleaseScratch(void);
 
+/* on != 0: every solve call (the strided-batch, batched, ragged, ADI,
+ * adjoint and mixed entry points) pushes an NVTX range named after itself
+ * for its host-side duration, so Nsight Systems timelines and ncu
+ * --nvtx-include filters can pick out the library's calls. Off by default,
+ * or on from the first call when TRIDSOLVER_NVTX=1 is set in the
+ * environment. Counterpart of the reference's NVTX profiling ranges
+ * (BEGIN_PROFILING, scalar/include/cuda_timing.h:58-102), which are chosen
+ * at build time there. */
+EXTERN_C tridStatus_t tridSetTracing(int on);
+
 /* ---- plan selection ------------------------------------------------------
  * Kernel families, chosen per system length by the built-in table or the
  * autotuner:

@@ -133,6 +133,19 @@ def test_empty_problem_is_success_without_device():
     assert st == TridStatus.SUCCESS
 
 
+def test_tracing_ranges_wrap_calls():
+    """With NVTX tracing on, calls still answer as before (the ranges are
+    host-side and need no device)."""
+    tb.set_tracing(True)
+    try:
+        st = tb.tridDmtsvStridedBatch(None, None, 4096, 4096, 4096, 1, 0, [8], [8])
+        assert st == TridStatus.INVALID_VALUE
+        st = tb.tridSmtsvStridedBatchInc(None, None, None, None, None, None, 2, 1, [0, 5], [0, 5])
+        assert st == TridStatus.SUCCESS
+    finally:
+        tb.set_tracing(False)
+
+
 def test_release_scratch_reports_missing_device():
     """Without a usable device the release returns an error status (raised
     as TridError), it does not crash."""

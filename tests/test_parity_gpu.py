@@ -264,6 +264,21 @@ def test_contiguous_reciprocal_within_one_ulp(n, dt, emax):
     assert st == tb.TridStatus.ZERO_PIVOT
 
 
+def test_solve_with_tracing_on(oracle):
+    """NVTX ranges around the calls change nothing in the results."""
+    dims, sd = [64, 48, 40], 2
+    a, b, c, d = make_system(dims, sd, np.float64, seed=11)
+    tb.set_tracing(True)
+    try:
+        st, out, _ = run_gpu(a, b, c, d, dims, sd)
+    finally:
+        tb.set_tracing(False)
+    assert st == 0
+    want = d.copy()
+    oracle.strided_batch(a, b, c, want, dims, sd)
+    assert normwise(out, want) <= 1e-12
+
+
 def test_async_stream_matches_blocking(oracle):
     dims, sd = [64, 48, 40], 1
     a, b, c, d = make_system(dims, sd, np.float64, seed=9)

@@ -35,6 +35,7 @@ SYMBOLS = {
     "tridGetPivotStatus": (_I, []),
     "tridGetLaunchCount": (ctypes.c_ulonglong, []),
     "tridReleaseScratch": (_I, []),
+    "tridSetTracing": (_I, [_I]),
     "tridForcePlan": (_I, [_I, _I]),
     "tridForceSystemsPerBlock": (_I, [_I]),
     "tridForceTma": (_I, [_I]),

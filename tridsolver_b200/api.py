@@ -194,6 +194,11 @@ def launch_count():
     return int(_lib.load().tridGetLaunchCount())
 
 
+def set_tracing(on=True):
+    """NVTX ranges around the library's solve calls (tridSetTracing)."""
+    _lib.load().tridSetTracing(1 if on else 0)
+
+
 def release_scratch():
     """Return the unused memory of the library's scratch pool on the current
     device to the driver (tridReleaseScratch)."""

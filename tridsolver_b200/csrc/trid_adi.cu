@@ -198,11 +198,13 @@ using namespace trid;
 EXTERN_C tridStatus_t tridDADIStep(double *u, double *du, double *a, double *b, double *c,
                                    const double *lam, int *step, double alpha, int nx, int ny,
                                    int nz) {
+  const TraceScope trace("tridDADIStep");
   return adi_step<double>(u, du, a, b, c, lam, step, alpha, nx, ny, nz);
 }
 
 EXTERN_C tridStatus_t tridSADIStep(float *u, float *du, float *a, float *b, float *c,
                                    const float *lam, int *step, float alpha, int nx, int ny,
                                    int nz) {
+  const TraceScope trace("tridSADIStep");
   return adi_step<float>(u, du, a, b, c, lam, step, alpha, nx, ny, nz);
 }

@@ -243,6 +243,7 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchAdjoint(const TridParams *ctx, const 
                                                    double *abar, double *bbar, double *cbar,
                                                    int ndim, int solvedim, const int *dims,
                                                    const int *pads) {
+  const TraceScope trace("tridDmtsvStridedBatchAdjoint");
   return adjoint<double>(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndim, solvedim, dims, pads);
 }
 
@@ -251,5 +252,6 @@ EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const TridParams *ctx, const 
                                                    const float *w, float *dbar, float *abar,
                                                    float *bbar, float *cbar, int ndim,
                                                    int solvedim, const int *dims, const int *pads) {
+  const TraceScope trace("tridSmtsvStridedBatchAdjoint");
   return adjoint<float>(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndim, solvedim, dims, pads);
 }

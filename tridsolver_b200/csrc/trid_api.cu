@@ -3,7 +3,10 @@
 // include/tridsolver_b200.h.
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -65,6 +68,30 @@ bool pivot_flag_take() {
   unsigned v = *w;
   if (v) *w = 0u;
   return v != 0;
+}
+
+// ---- NVTX ranges -------------------------------------------------------------
+namespace {
+std::atomic<int> g_trace{-1};  // -1: not decided yet (read the environment)
+}  // namespace
+
+static bool tracing_on() {
+  int v = g_trace.load(std::memory_order_relaxed);
+  if (v < 0) {
+    const char *env = getenv("TRIDSOLVER_NVTX");
+    int undecided = -1;
+    g_trace.compare_exchange_strong(undecided, env && env[0] && env[0] != '0' ? 1 : 0);
+    v = g_trace.load(std::memory_order_relaxed);
+  }
+  return v > 0;
+}
+
+TraceScope::TraceScope(const char *name) : on_(tracing_on()) {
+  if (on_) nvtxRangePushA(name);
+}
+
+TraceScope::~TraceScope() {
+  if (on_) nvtxRangePop();
 }
 
 // ---- device check ----------------------------------------------------------
@@ -260,6 +287,7 @@ EXTERN_C tridStatus_t tridDsolveBatchedTrid(const TridParams *ctx, int numTrids,
                                             int stride1, int stride2, int subBatchSize,
                                             int subBatchStride, const double *a, const double *b,
                                             const double *c, const double *d, double *x) {
+  const TraceScope trace("tridDsolveBatchedTrid");
   return solve_batched<double, false>(ctx, numTrids, length, stride1, stride2, subBatchSize,
                                       subBatchStride, a, b, c, d, x);
 }
@@ -268,6 +296,7 @@ EXTERN_C tridStatus_t tridSsolveBatchedTrid(const TridParams *ctx, int numTrids,
                                             int stride1, int stride2, int subBatchSize,
                                             int subBatchStride, const float *a, const float *b,
                                             const float *c, const float *d, float *x) {
+  const TraceScope trace("tridSsolveBatchedTrid");
   return solve_batched<float, false>(ctx, numTrids, length, stride1, stride2, subBatchSize,
                                      subBatchStride, a, b, c, d, x);
 }
@@ -277,6 +306,7 @@ EXTERN_C tridStatus_t tridDsolveBatchedTridInc(const TridParams *ctx, int numTri
                                                int subBatchStride, const double *a,
                                                const double *b, const double *c, const double *d,
                                                double *x) {
+  const TraceScope trace("tridDsolveBatchedTridInc");
   return solve_batched<double, true>(ctx, numTrids, length, stride1, stride2, subBatchSize,
                                      subBatchStride, a, b, c, d, x);
 }
@@ -285,6 +315,7 @@ EXTERN_C tridStatus_t tridSsolveBatchedTridInc(const TridParams *ctx, int numTri
                                                int stride1, int stride2, int subBatchSize,
                                                int subBatchStride, const float *a, const float *b,
                                                const float *c, const float *d, float *x) {
+  const TraceScope trace("tridSsolveBatchedTridInc");
   return solve_batched<float, true>(ctx, numTrids, length, stride1, stride2, subBatchSize,
                                     subBatchStride, a, b, c, d, x);
 }
@@ -292,12 +323,14 @@ EXTERN_C tridStatus_t tridSsolveBatchedTridInc(const TridParams *ctx, int numTri
 EXTERN_C tridStatus_t tridDmtsvStridedBatch(const TridParams *ctx, const double *a, const double *b,
                                             const double *c, double *d, int ndim, int solvedim,
                                             const int *dims, const int *pads) {
+  const TraceScope trace("tridDmtsvStridedBatch");
   return solve_strided<double, false>(ctx, a, b, c, d, nullptr, ndim, solvedim, dims, pads);
 }
 
 EXTERN_C tridStatus_t tridSmtsvStridedBatch(const TridParams *ctx, const float *a, const float *b,
                                             const float *c, float *d, int ndim, int solvedim,
                                             const int *dims, const int *pads) {
+  const TraceScope trace("tridSmtsvStridedBatch");
   return solve_strided<float, false>(ctx, a, b, c, d, nullptr, ndim, solvedim, dims, pads);
 }
 
@@ -305,6 +338,7 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const TridParams *ctx, const doub
                                                const double *b, const double *c, double *d,
                                                double *u, int ndim, int solvedim, const int *dims,
                                                const int *pads) {
+  const TraceScope trace("tridDmtsvStridedBatchInc");
   return solve_strided<double, true>(ctx, a, b, c, d, u, ndim, solvedim, dims, pads);
 }
 
@@ -312,6 +346,7 @@ EXTERN_C tridStatus_t tridSmtsvStridedBatchInc(const TridParams *ctx, const floa
                                                const float *b, const float *c, float *d, float *u,
                                                int ndim, int solvedim, const int *dims,
                                                const int *pads) {
+  const TraceScope trace("tridSmtsvStridedBatchInc");
   return solve_strided<float, true>(ctx, a, b, c, d, u, ndim, solvedim, dims, pads);
 }
 
@@ -338,6 +373,11 @@ EXTERN_C tridStatus_t tridGetPivotStatus(void) {
 EXTERN_C unsigned long long tridGetLaunchCount(void) { return g_launches.load(); }
 
 EXTERN_C tridStatus_t tridReleaseScratch(void) { return status_of(scratch_release()); }
+
+EXTERN_C tridStatus_t tridSetTracing(int on) {
+  g_trace.store(on ? 1 : 0, std::memory_order_relaxed);
+  return TRID_STATUS_SUCCESS;
+}
 
 EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread) {
   Settings &s = settings();

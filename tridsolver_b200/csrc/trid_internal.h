@@ -43,6 +43,21 @@ cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t st);
 cudaError_t scratch_free(void *ptr, cudaStream_t st);
 cudaError_t scratch_release();
 
+// An NVTX range named after one library call, for Nsight Systems timelines
+// and ncu range filters, while tracing is on (tridSetTracing, or
+// TRIDSOLVER_NVTX=1 in the environment at the first call); nothing
+// otherwise. Ranges are per host thread.
+class TraceScope {
+ public:
+  explicit TraceScope(const char *name);
+  ~TraceScope();
+  TraceScope(const TraceScope &) = delete;
+  TraceScope &operator=(const TraceScope &) = delete;
+
+ private:
+  bool on_;
+};
+
 // Host-mapped zero-pivot word of the current device (device pointer), or
 // nullptr if it could not be set up.
 unsigned *pivot_flag_device();

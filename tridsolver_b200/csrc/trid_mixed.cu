@@ -738,6 +738,7 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
                                                  int ndim, int solvedim, const int *dims_p,
                                                  const int *pads_p, int max_iters, double tol,
                                                  int *iters_out, double *correction_out) {
+  const TraceScope trace("tridDmtsvStridedBatchMixed");
   (void)ctx;
   if (iters_out) *iters_out = -1;
   if (correction_out) *correction_out = -1.0;

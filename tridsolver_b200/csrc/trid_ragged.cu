@@ -754,6 +754,7 @@ using namespace trid;
 EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *a, const double *b,
                                            const double *c, double *d, const int64_t *offsets,
                                            long long nsys) {
+  const TraceScope trace("tridDmtsvRaggedBatch");
   (void)ctx;
   return ragged<double>(a, b, c, d, offsets, nsys);
 }
@@ -761,6 +762,7 @@ EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *
 EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a, const float *b,
                                            const float *c, float *d, const int64_t *offsets,
                                            long long nsys) {
+  const TraceScope trace("tridSmtsvRaggedBatch");
   (void)ctx;
   return ragged<float>(a, b, c, d, offsets, nsys);
 }
