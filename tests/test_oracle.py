@@ -142,3 +142,42 @@ def test_invalid_arguments_rejected(restatement):
     a, b, c, d = make_system([4, 4], 0)
     with pytest.raises(ValueError):
         restatement.strided_batch(a, b, c, d, [4, 4], 2)
+
+
+try:
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as hs
+except ImportError:  # pragma: no cover
+    given = None
+
+
+if given is not None:
+    @settings(max_examples=80, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(data=hs.data())
+    def test_fuzz_restatement_against_reference(data, restatement, reference):
+        """Random shapes, system directions, paddings (pointer at the first
+        interior element, as scalar/test/test_cpu.cpp:86-128 does), Inc and
+        precision: the restatement and the reference's own library agree on
+        the interior, and Inc leaves d as it was."""
+        ndim = data.draw(hs.integers(1, 3))
+        dims = [data.draw(hs.integers(1, 24)) for _ in range(ndim)]
+        solvedim = data.draw(hs.integers(0, ndim - 1))
+        pads = [n + data.draw(hs.integers(0, 2)) for n in dims]
+        inc = data.draw(hs.booleans())
+        dt = data.draw(hs.sampled_from(DTYPES))
+        seed = data.draw(hs.integers(0, 2 ** 31 - 1))
+        a, b, c, d = make_system(dims, solvedim, dt, seed=seed)
+        u0 = np.random.default_rng(seed + 1).standard_normal(d.size).astype(dt) if inc else None
+        off = pad_offset(pads)
+        outs = []
+        for lib in (restatement, reference):
+            arrs = [to_padded(v, dims, pads, fill=3.0) for v in (a, b, c, d)]
+            up = to_padded(u0, dims, pads, fill=3.0) if inc else None
+            lib.strided_batch(*(v[off:] for v in arrs), dims, solvedim, pads=pads,
+                              u=up[off:] if inc else None)
+            got = from_padded(up if inc else arrs[3], dims, pads)
+            outs.append(got)
+            if inc:
+                assert np.array_equal(from_padded(arrs[3], dims, pads), d)
+        tol = 1e-13 if dt == np.float64 else 2e-6
+        assert normwise(outs[0], outs[1]) <= tol, (dims, solvedim, pads, inc, dt)
