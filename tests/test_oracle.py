@@ -220,3 +220,39 @@ def test_adi_oracle_matches_reference_solves(shape, dt, restatement, reference):
     reference.strided_batch(a, b, c, d, dims, 2, u=u_ref)
     tol = 1e-13 if dt == np.float64 else 2e-6
     assert normwise(u_oracle, u_ref) <= tol
+
+
+@pytest.mark.parametrize("dims,sd", [([12, 7, 5], 0), ([6, 20, 5], 1), ([5, 6, 17], 2), ([40], 0)])
+def test_adjoint_oracle_against_reference_transposed_solve(dims, sd, restatement, reference):
+    """The adjoint oracle against a gradient built from the reference's own
+    CPU solver: dbar solves T^T dbar = w, which is the tridiagonal system
+    with sub-diagonal c one row up and super-diagonal a one row down; then
+    abar_i = -dbar_i x_{i-1}, bbar_i = -dbar_i x_i, cbar_i = -dbar_i x_{i+1}."""
+    a, b, c, d = make_system(dims, sd, np.float64, seed=sum(dims) + sd)
+    w = np.random.default_rng(5).standard_normal(d.size)
+    x = d.copy()
+    reference.strided_batch(a, b, c, x, dims, sd)
+    abar, bbar, cbar, dbar = restatement.adjoint(a, b, c, x, w, dims, sd)
+
+    shape = tuple(reversed(dims))
+    ax = len(dims) - 1 - sd
+    first = [slice(None)] * len(dims)
+    first[ax] = 0
+    last = [slice(None)] * len(dims)
+    last[ax] = -1
+    A, C, X = (v.reshape(shape) for v in (a, c, x))
+    at = np.roll(C, 1, axis=ax)
+    at[tuple(first)] = 0.0
+    ct = np.roll(A, -1, axis=ax)
+    ct[tuple(last)] = 0.0
+    dref = w.copy()
+    reference.strided_batch(at.ravel().copy(), b, ct.ravel().copy(), dref, dims, sd)
+    Dr = dref.reshape(shape)
+    xm = np.roll(X, 1, axis=ax)
+    xm[tuple(first)] = 0.0
+    xp = np.roll(X, -1, axis=ax)
+    xp[tuple(last)] = 0.0
+    want = {"abar": (-Dr * xm).ravel(), "bbar": (-Dr * X).ravel(), "cbar": (-Dr * xp).ravel(),
+            "dbar": dref}
+    for name, got in (("abar", abar), ("bbar", bbar), ("cbar", cbar), ("dbar", dbar)):
+        assert normwise(got, want[name]) <= 1e-13, name
