@@ -265,3 +265,24 @@ def test_adjoint_oracle_against_reference_transposed_solve(dims, sd, restatement
             "dbar": dref}
     for name, got in (("abar", abar), ("bbar", bbar), ("cbar", cbar), ("dbar", dbar)):
         assert normwise(got, want[name]) <= 1e-13, name
+
+
+if given is not None:
+    @settings(max_examples=100, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(n=hs.integers(1, 40), seed=hs.integers(0, 2 ** 31 - 1))
+    def test_fuzz_restatement_against_dense_solve(n, seed, restatement):
+        """One system against numpy's dense LU solve of the same matrix, a
+        check independent of both Thomas implementations (a[0] and c[n-1]
+        are outside the matrix and must not matter)."""
+        rng = np.random.default_rng(seed)
+        a = rng.uniform(-0.5, 0.5, n)
+        c = rng.uniform(-0.5, 0.5, n)
+        b = 1 + np.abs(a) + np.abs(c) + rng.uniform(0, 1, n)
+        d = rng.standard_normal(n)
+        a[0] = rng.uniform(-5, 5)
+        c[-1] = rng.uniform(-5, 5)
+        T = np.diag(b) + np.diag(a[1:], -1) + np.diag(c[:-1], 1)
+        want = np.linalg.solve(T, d)
+        got = d.copy()
+        restatement.strided_batch(a, b, c, got, [n], 0)
+        assert normwise(got, want) <= 1e-13
