@@ -77,10 +77,13 @@ EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);
  * per-thread loads, which measure faster for rows of 32-64 bytes. */
 EXTERN_C tridStatus_t tridForceTma(int mode);
 
-/* Strided batches of 64 < N <= 512 rows: -1 (default) = the persistent
- * streaming kernel (groups of 128 bytes of neighbouring systems, loads kept
- * in flight across groups) unless TMA is forced; 1 = always that kernel where
- * it applies; 0 = the register-tile strided kernel. */
+/* Strided batches of 64 < N <= 512 rows: -1 (default) = automatic: the wide
+ * streaming kernel (groups of 256 bytes of neighbouring systems, elimination
+ * state parked in tensor memory) when rows are at least 64 KiB apart (z
+ * solves), else the persistent streaming kernel (groups of 128 bytes, loads
+ * kept in flight across groups), unless TMA is forced; 1 = the 128-byte
+ * streaming kernel and 2 = the wide one, wherever they apply; 0 = the
+ * register-tile strided kernel. */
 EXTERN_C tridStatus_t tridForceStream(int mode);
 
 /* ---- ragged batches -------------------------------------------------------

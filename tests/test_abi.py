@@ -160,9 +160,11 @@ def test_release_scratch_reports_missing_device():
 
 @pytest.mark.parametrize("dtype_bytes,dims,solvedim,expect", [
     (8, [512, 512, 512], 0, "hybrid M=16 T=32 W=1 smem"),
-    (8, [512, 512, 512], 2, "hybrid M=16 T=32 W=16 stream"),
+    (8, [512, 512, 512], 2, "hybrid M=32 T=16 W=32 wide"),
     (8, [512, 512, 512], 1, "hybrid M=16 T=32 W=16 stream"),
-    (8, [256, 256, 256], 2, "hybrid M=8 T=32 W=16 stream"),
+    (8, [256, 256, 256], 2, "hybrid M=16 T=16 W=32 wide"),
+    (8, [16, 512, 300], 2, "hybrid M=32 T=16 W=32 wide"),
+    (8, [15, 512, 300], 2, "hybrid M=16 T=32 W=16 stream"),
     (8, [7, 512, 3], 1, "hybrid M=8 T=64 W=8"),
     (8, [8, 512, 3], 1, "hybrid M=16 T=32 W=16 stream"),
     (4, [512, 512, 512], 2, "hybrid M=16 T=32 W=32 stream"),

@@ -202,14 +202,16 @@ def test_tma_tiles(dims, solvedim, tma, inc, dt, oracle, reference):
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 @pytest.mark.parametrize("inc", [False, True])
-@pytest.mark.parametrize("stream", [1, 0])
+@pytest.mark.parametrize("stream", [2, 1, 0])
 @pytest.mark.parametrize("dims,solvedim", [([48, 37, 100], 2), ([24, 300, 3], 1), ([20, 3, 260], 2),
                                            ([7, 130, 5], 1), ([64, 65], 1), ([5, 9, 512], 2),
-                                           ([33, 17, 129], 2), ([40, 257], 1)])
+                                           ([33, 17, 129], 2), ([40, 257], 1), ([70, 3, 300], 2),
+                                           ([96, 2, 511], 2), ([200, 129], 1)])
 def test_streaming_kernel(dims, solvedim, stream, inc, dt, oracle, reference):
-    """Persistent streaming strided kernel against the register-tile kernel
-    and the oracle: partial groups, every chunk size (M = 4, 8, 16), lengths
-    that end inside a chunk, groups fewer than the grid and many per CTA."""
+    """Persistent streaming strided kernels (2: 256-byte groups with the state
+    in tensor memory, 1: 128-byte groups) against the register-tile kernel
+    and the oracle: partial groups, every chunk size, lengths that end inside
+    a chunk, groups fewer than the grid and many per CTA."""
     tb.force_stream(stream)
     try:
         _check(dims, solvedim, dt, inc, oracle, reference, seed=3 + stream + 2 * inc)

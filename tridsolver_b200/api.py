@@ -227,8 +227,11 @@ def force_tma(mode=-1):
 
 
 def force_stream(mode=-1):
-    """Strided batches of 64 < N <= 512: -1 (default) streaming kernel unless
-    TMA is forced, 1 always where it applies, 0 the register-tile kernel."""
+    """Strided batches of 64 < N <= 512: -1 (default) automatic (the wide
+    streaming kernel with 256-byte groups for rows a plane apart, else the
+    streaming kernel with 128-byte groups, unless TMA is forced); 1 the
+    128-byte streaming kernel, 2 the wide one, wherever they apply; 0 the
+    register-tile kernel."""
     st = _lib.load().tridForceStream(int(mode))
     if st != 0:
         raise TridError(st, "tridForceStream")

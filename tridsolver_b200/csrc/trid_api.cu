@@ -409,7 +409,7 @@ EXTERN_C tridStatus_t tridForceTma(int mode) {
 }
 
 EXTERN_C tridStatus_t tridForceStream(int mode) {
-  if (mode < -1 || mode > 1) return TRID_STATUS_INVALID_VALUE;
+  if (mode < -1 || mode > 2) return TRID_STATUS_INVALID_VALUE;
   settings().force_stream = mode;
   return TRID_STATUS_SUCCESS;
 }

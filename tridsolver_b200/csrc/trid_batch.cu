@@ -13,7 +13,7 @@ std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
   snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
-           smem ? " smem" : vec ? " vec" : tma ? " tma" : streaming ? " stream" : "");
+           smem ? " smem" : vec ? " vec" : tma ? " tma" : wide ? " wide" : streaming ? " stream" : "");
   return buf;
 }
 
@@ -106,13 +106,30 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         const int fs = honour_force ? st.force_stream : -1;
         const bool want_tma = honour_force && st.force_tma == 1;
         const int fm = honour_force ? st.force_m : 0;
+        // the wide form (256-byte groups, state in tensor memory) for FP64
+        // rows a whole plane apart (>= 64 KiB: z solves), where the rate of
+        // row segments limits 128-byte groups (512^3 z: 0.88 vs 1.11 ms, Inc
+        // 1.05 vs 1.47 ms), when at least half a group holds systems. Along y
+        // the 128-byte form with L2 prefetch measured faster (0.85 vs 0.87
+        // ms), and so did FP32 (whose 512-thread wide CTA has half the bytes
+        // in flight). Forced with tridForceStream(2) wherever it applies.
+        const int mw = wide_rows_per_thread<R>(N);
+        const bool zlike = p.stride * (long long)sizeof(R) >= (1LL << 16);
+        if (mw > 0 && fm == 0 && !want_tma &&
+            (fs == 2 || (fs == -1 && sizeof(R) == 8 && zlike && 2 * p.n0 >= wide_width<R>()))) {
+          plan.M = mw;
+          plan.T = 512 / wide_width<R>();
+          plan.W = wide_width<R>();
+          plan.wide = true;
+          return plan;
+        }
         const int Ts = 32;
         const int m_lo = 4;  // instantiated: 4, 8, 16
         const bool fm_ok = fm == 0 || ((fm == m_lo || fm == 2 * m_lo || fm == 4 * m_lo) && Ts * fm >= N);
         // (groups are always 128 bytes wide: automatic only when at least half
         // of a group holds systems)
         const int Ws = stream_width<R>(p.n0);
-        if ((fs == 1 || (fs == -1 && !want_tma && fm_ok && 2 * p.n0 >= Ws)) && N > 64 && N <= 512) {
+        if ((fs >= 1 || (fs == -1 && !want_tma && fm_ok && 2 * p.n0 >= Ws)) && N > 64 && N <= 512) {
           int Ms = N <= Ts * m_lo ? m_lo : N <= 2 * Ts * m_lo ? 2 * m_lo : 4 * m_lo;
           int Tsel = Ts;
           if (fm > 0 && fm_ok) {
@@ -312,7 +329,14 @@ cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t s
     case TRID_FAMILY_PCR: return launch_pcr<R, INC>(p, plan, st);
     case TRID_FAMILY_LONG:
       return plan.M == 8 ? launch_long_m<R, 8, INC>(p, st) : launch_long_m<R, 16, INC>(p, st);
-    default: return launch_hybrid<R, INC>(p, plan, st);
+    default:
+      if (plan.wide) {
+        // rows per thread up to 64 (FP32), chosen inside the launcher
+        const cudaError_t e = launch_strided_wide<R, INC>(p, st);
+        if (e == cudaSuccess) g_launches.fetch_add(1, std::memory_order_relaxed);
+        return e;
+      }
+      return launch_hybrid<R, INC>(p, plan, st);
   }
 }
 

@@ -20,6 +20,7 @@ struct Plan {
   bool smem = false;                // warp-per-system staging through shared memory
   bool tma = false;                 // strided: TMA tiles, persistent, double-buffered
   bool streaming = false;           // strided: persistent streaming kernel (T = 32)
+  bool wide = false;                // strided: wide streaming kernel (256-byte groups)
   std::string describe() const;
 };
 
@@ -31,7 +32,7 @@ struct Settings {
   int force_m = 0;
   int force_w = 0;
   int force_tma = -1;  // -1 automatic, 0 off, 1 on where it applies
-  int force_stream = -1;  // -1 automatic, 0 off, 1 on where it applies
+  int force_stream = -1;  // -1 automatic, 0 off, 1 128-byte groups, 2 256-byte groups
   int mixed_mode = 0;     // tridSetMixedMode: 0 automatic, 1 refinement, 2 promoted
 };
 Settings &settings();
@@ -94,6 +95,13 @@ cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOu
                                           cudaStream_t st);
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
+// Wide streaming kernel (trid_strided_wide.cu): 256-byte groups with the
+// elimination state parked in tensor memory; rows per thread for N rows
+// (0 when it does not apply), group width, launcher.
+template <typename R> int wide_rows_per_thread(int N);
+template <typename R> int wide_width();
+template <typename R, bool INC>
+cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st);
 // The streaming kernel in FP64 arithmetic on FP32-stored a, b, c.
 template <int M>
 cudaError_t launch_strided_stream_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,

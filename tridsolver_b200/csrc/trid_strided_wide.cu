@@ -1,0 +1,392 @@
+// Strided batches (solvedim >= 1) of 64 < N <= 512 rows: the wide streaming
+// kernel, groups of 256 bytes of neighbouring systems.
+//
+// Why wider groups: when the rows of a system are a whole plane apart (z
+// solves), every row of a group is a separate memory segment on its own
+// page, and the rate of such segments, not the bytes, limits the solve. An
+// access probe with the solve's pattern (4 arrays read, 1 written, 512^3
+// FP64, rows 2 MiB apart) measured 4.6-5.3 TB/s with 128-byte segments at
+// any window depth and 6.5-6.8 TB/s with 256-byte ones.
+//
+// A 256-byte group of 512-row systems carries 384 KiB of elimination state
+// (a', c', d' of every row), more than shared memory holds. So:
+//   - a' and c' of every row go to tensor memory (TMEM, 128 lanes x 512
+//     columns of 32 bits per SM): the CTA allocates all 512 columns once,
+//     and each warp keeps its rows in its lane quarter (warp w: lanes
+//     32 (w % 4) .. + 31, columns (w / 4) * 128 .. + 127, i.e. 128 32-bit
+//     words per thread: 32 FP64 rows or 64 FP32 rows of a' and c');
+//   - d' goes to the thread's private shared-memory slots [j * BS + tid];
+//   - the chunk's top reduced row is accumulated in forward order during the
+//     forward sweep (x_1 = P + Q x_0 + S x_{k+1} as rows k are eliminated), so
+//     the parked state is read back once, by the back-substitution.
+// The CTA (512 threads; W systems x T chunks, thread (s, t) = (tid % W,
+// tid / W)) is persistent and walks over groups; each thread streams its
+// chunk's rows through a D-deep register window that runs on into the next
+// group, so loads stay in flight across the reduced solve and the stores.
+// The dynamic shared memory request is at least 120 KiB, so one CTA runs per
+// SM and the 512-column allocation never waits for another CTA of this
+// kernel. Every path through the kernel reaches the deallocation at its end.
+//
+// Inc variants load u block by block during the back-substitution (one
+// block ahead, the first block before the reduced solve).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "trid_internal.h"
+
+namespace trid {
+
+namespace {
+
+template <typename R> constexpr int wide_w() { return 256 / (int)sizeof(R); }
+// chunks per system: 16 FP64 (32 systems x 16 = 512 threads), 8 FP32
+template <typename R> constexpr int wide_t() { return sizeof(R) == 8 ? 16 : 8; }
+template <typename R> constexpr int wide_bs() { return wide_w<R>() * wide_t<R>(); }
+// 32-bit TMEM columns per row: a' and c'
+template <typename R> constexpr int wide_cpr() { return 2 * (int)sizeof(R) / 4; }
+// rows per back-substitution block (one TMEM load of 32 columns; 16 for Inc)
+template <typename R, bool INC> constexpr int wide_blk() { return (INC ? 16 : 32) / wide_cpr<R>(); }
+constexpr int WIDE_SMEM_MIN = 120 * 1024;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void tmem_alloc_all(uint32_t *slot) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(slot))
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_all(uint32_t base) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(base) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+
+// one row's a', c' into this thread's lane at column `col`
+__device__ __forceinline__ void tmem_put_row(uint32_t taddr, double af, double cf) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr),
+               "r"(__double2loint(af)), "r"(__double2hiint(af)), "r"(__double2loint(cf)),
+               "r"(__double2hiint(cf))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_put_row(uint32_t taddr, float af, float cf) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n" ::"r"(taddr), "r"(__float_as_uint(af)),
+               "r"(__float_as_uint(cf))
+               : "memory");
+}
+
+// 16 or 32 consecutive columns of this thread's lane (then tmem_wait_ld)
+__device__ __forceinline__ void tmem_get(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+      "[%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+        "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+        "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+        "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_get(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+        "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+// Waits for this thread's TMEM loads. The loaded registers are in/out
+// operands, so no use of them can be scheduled above the wait.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
+               :
+               : "memory");
+}
+
+// a', c' of row i of a block loaded by tmem_get
+template <typename R, int NW>
+__device__ __forceinline__ void tmem_row(const uint32_t (&v)[NW], int i, R &af, R &cf) {
+  if constexpr (sizeof(R) == 8) {
+    af = __hiloint2double((int)v[4 * i + 1], (int)v[4 * i]);
+    cf = __hiloint2double((int)v[4 * i + 3], (int)v[4 * i + 2]);
+  } else {
+    af = __uint_as_float(v[2 * i]);
+    cf = __uint_as_float(v[2 * i + 1]);
+  }
+}
+
+// Row `row` at element offset o: identity rows outside the system, a[0] and
+// c[N-1] forced to zero. Loads are cached in L2 only: nothing is read twice.
+template <typename R, bool INC>
+__device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, long long o, bool valid, int row, R &a,
+                                              R &b, R &c, R &d) {
+  if (valid) {
+    a = row == 0 ? R(0) : __ldcg(p.a + o);
+    c = row == p.N - 1 ? R(0) : __ldcg(p.c + o);
+    b = __ldcg(p.b + o);
+    d = __ldcg(p.d_in + o);
+  } else {
+    a = R(0);
+    b = R(1);
+    c = R(0);
+    d = R(0);
+  }
+}
+
+}  // namespace
+
+template <typename R, int M, int D, bool INC>
+__global__ void __launch_bounds__(wide_bs<R>(), 1)
+    strided_wide_kernel(const BatchArgs<R> p, long long ngx, long long ngroups) {
+  constexpr int W = wide_w<R>();
+  constexpr int T = wide_t<R>();
+  constexpr int BS = W * T;
+  constexpr int NWARP = BS / 32;
+  constexpr int CW = 512 / (NWARP / 4);  // TMEM columns per warp
+  constexpr int CPR = wide_cpr<R>();
+  constexpr int B = wide_blk<R, INC>() < M ? wide_blk<R, INC>() : M;
+  constexpr int NV = B * CPR;
+  static_assert(NV == 16 || NV == 32, "one TMEM load per block");
+  static_assert(NWARP % 4 == 0, "whole lane quarters");
+  static_assert(M * CPR <= CW, "a' and c' of a chunk fit the warp's TMEM columns");
+  static_assert(M % B == 0 && M % D == 0 && D <= M && M >= 4, "blocks and window tile the chunk");
+  constexpr int RED = (6 * T * (W + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
+  extern __shared__ __align__(16) unsigned char wide_smem[];
+  __shared__ uint32_t tmem_slot;
+  R *red = reinterpret_cast<R *>(wide_smem);
+  const int tid = threadIdx.x;
+  R *sdf = red + RED + tid;  // d' of row j at [j * BS]
+  const int s = tid % W;
+  const int t = tid / W;
+  const int warp = tid >> 5;
+  const int N = p.N;
+  const int row0 = t * M;
+  const long long stride = p.stride;
+
+  if (warp == 0) tmem_alloc_all(&tmem_slot);
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t tbase = tmem_slot;
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * CW);
+
+  auto group_first = [&](long long g, bool &act) -> long long {
+    const long long gx = g % ngx;
+    const long long i1 = g / ngx;
+    const long long i0 = gx * W + s;
+    act = g < ngroups && i0 < p.n0;
+    return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
+  };
+
+  R pa[D], pb[D], pc[D], pd[D];
+  long long g = blockIdx.x;
+  bool act;
+  long long first = group_first(g, act);
+  long long lo = first;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    wide_load_row<R, INC>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
+    lo += stride;
+  }
+
+  bool bad = false;
+  for (; g < ngroups; g += gridDim.x) {
+    bool actn;
+    const long long firstn = group_first(g + gridDim.x, actn);
+    long long ln = firstn;
+
+    // forward half of the chunk elimination, streamed row by row; the top
+    // reduced row accumulates as x_1 = P + Q x_0 + S x_{j+1}
+    R ap = R(0), cp = R(0), dp = R(0);
+    R a0 = R(0), c0 = R(0), d0 = R(0);
+    R P = R(0), Q = R(0), S = R(1);
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int k = j % D;
+      const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
+      if (j + D < M) {
+        const int row = row0 + j + D;
+        wide_load_row<R, INC>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        lo += stride;
+      } else {
+        const int row = row0 + j + D - M;
+        wide_load_row<R, INC>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        ln += stride;
+      }
+      R af, cf, df;
+      if (j < 2) {
+        const R r = rcp(b);
+        bad |= !finite_rcp(r);
+        af = a * r;
+        cf = c * r;
+        df = d * r;
+      } else {
+        const R r = rcp(b - a * cp);
+        bad |= !finite_rcp(r);
+        df = r * (d - a * dp);
+        af = -r * a * ap;
+        cf = r * c;
+      }
+      tmem_put_row(taddr + (uint32_t)(j * CPR), af, cf);
+      sdf[j * BS] = df;
+      if (j == 0) {
+        a0 = af;
+        c0 = cf;
+        d0 = df;
+      } else if (j <= M - 2) {
+        P += S * df;
+        Q -= S * af;
+        S = -S * cf;
+      }
+      ap = af;
+      cp = cf;
+      dp = df;
+    }
+    const R r0 = rcp(R(1) + c0 * Q);
+    bad |= !finite_rcp(r0);
+    const Row<R> top{r0 * a0, r0 * c0 * S, r0 * (d0 - c0 * P)};
+    const Row<R> bot{ap, cp, dp};
+
+    // Inc: u of the last block, in flight during the reduced solve
+    long long o = first + (long long)(M - 1) * stride;
+    R ucur[INC ? B : 1], unext[INC ? B : 1];
+    if constexpr (INC) {
+#pragma unroll
+      for (int i = 0; i < B; ++i) {
+        const int j = M - 1 - i;
+        ucur[i] = (act && row0 + j < N) ? __ldcg(p.u + o - (long long)i * stride) : R(0);
+      }
+    }
+    tmem_wait_st();
+    R y, z;
+    block_reduced_solve<R, 2>(red, top, bot, s, t, T, W, y, z, bad);
+
+    // back-substitution with the parked rows, block by block from the
+    // chunk's last row up, stored as it goes
+    R x = z;
+#pragma unroll
+    for (int bb = M / B - 1; bb >= 0; --bb) {
+      uint32_t v[NV];
+      tmem_get(taddr + (uint32_t)(bb * B * CPR), v);
+      if constexpr (INC) {
+        if (bb > 0) {
+#pragma unroll
+          for (int i = 0; i < B; ++i) {
+            const int j = bb * B - 1 - i;
+            unext[i] = (act && row0 + j < N) ? __ldcg(p.u + o - (long long)(B + i) * stride) : R(0);
+          }
+        }
+      }
+      tmem_wait_ld(v);
+#pragma unroll
+      for (int i = B - 1; i >= 0; --i) {
+        const int j = bb * B + i;
+        if (j < M - 1) {
+          if (j == 0) {
+            x = y;
+          } else {
+            R af, cf;
+            tmem_row<R, NV>(v, i, af, cf);
+            x = sdf[j * BS] - af * y - cf * x;
+          }
+        }
+        if (act && row0 + j < N) {
+          if constexpr (INC)
+            p.u[o] = ucur[B - 1 - i] + x;
+          else
+            p.d_out[o] = x;
+        }
+        o -= stride;
+      }
+      if constexpr (INC) {
+#pragma unroll
+        for (int i = 0; i < B; ++i) ucur[i] = unext[i];
+      }
+    }
+    first = firstn;
+    act = actn;
+    lo = ln;
+  }
+  report_bad_pivot(bad, p.flag);
+
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (warp == 0) tmem_dealloc_all(tbase);
+}
+
+template <typename R> int wide_width() { return wide_w<R>(); }
+
+// Rows per thread for a system of N rows (64 < N <= 512), 0 if none.
+template <typename R> int wide_rows_per_thread(int N) {
+  constexpr int T = wide_t<R>();
+  if (N <= 64 || N > 512) return 0;
+  if (N <= 8 * T) return 8;
+  if (N <= 16 * T) return 16;
+  if (N <= 32 * T) return 32;
+  return sizeof(R) == 4 && N <= 64 * T ? 64 : 0;
+}
+
+template <typename R, int M, bool INC>
+static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st) {
+  constexpr int W = wide_w<R>();
+  constexpr int T = wide_t<R>();
+  constexpr int BS = W * T;
+  constexpr int D = 4;
+  const size_t red = ((size_t)6 * T * (W + 1) * sizeof(R) + 15) / 16 * 16;
+  size_t smem = red + (size_t)M * BS * sizeof(R);
+  if (smem < (size_t)WIDE_SMEM_MIN) smem = WIDE_SMEM_MIN;  // one CTA per SM
+  auto kern = strided_wide_kernel<R, M, D, INC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long ngx = (p.n0 + W - 1) / W;
+  const long long ngroups = ngx * (p.nsys / p.n0);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long grid = ngroups < sms ? ngroups : sms;
+  kern<<<(unsigned)grid, BS, smem, st>>>(p, ngx, ngroups);
+  return cudaGetLastError();
+}
+
+template <typename R, bool INC>
+cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st) {
+  switch (wide_rows_per_thread<R>(p.N)) {
+    case 8: return launch_wide_m<R, 8, INC>(p, st);
+    case 16: return launch_wide_m<R, 16, INC>(p, st);
+    case 32: return launch_wide_m<R, 32, INC>(p, st);
+    case 64:
+      if constexpr (sizeof(R) == 4) return launch_wide_m<R, 64, INC>(p, st);
+      return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template cudaError_t launch_strided_wide<double, false>(const BatchArgs<double> &, cudaStream_t);
+template cudaError_t launch_strided_wide<double, true>(const BatchArgs<double> &, cudaStream_t);
+template cudaError_t launch_strided_wide<float, false>(const BatchArgs<float> &, cudaStream_t);
+template cudaError_t launch_strided_wide<float, true>(const BatchArgs<float> &, cudaStream_t);
+template int wide_width<double>();
+template int wide_width<float>();
+template int wide_rows_per_thread<double>(int);
+template int wide_rows_per_thread<float>(int);
+
+}  // namespace trid
