@@ -279,8 +279,11 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
  * stderr); systems short enough for one warp per system (N <= 512 along x,
  * N <= 1024 along y or z) need none. All calls share the array, so calls that
  * overlap on the GPU race; the first call on a device looks up the array's
- * address and should come before any stream capture. Zero pivots are
- * reported in blocking mode only. */
+ * address and should come before any stream capture, and a cudaDeviceReset
+ * after it is not supported. Zero pivots are reported in blocking mode only.
+ * The plan is always the automatic one (tridForce* settings are ignored), and
+ * a ctx whose mpi_params were registered by tridDistInit is refused with
+ * TRID_STATUS_INVALID_VALUE: the distributed solve is not available here. */
 EXTERN_C tridStatus_t tridDmtsvStridedBatchNoAlloc(const TridParams *ctx, const double *a,
                                                    const double *b, const double *c, double *d,
                                                    int ndim, int solvedim, const int *dims,

@@ -4,7 +4,7 @@ fixture generator, scalar/test/gen_testcases.py (seed pinned at :2).
 Run here, where the reference tree exists (it does not exist where the GPU
 tests run, which is why its output is committed):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 The generator draws a, b, c, d with numpy's legacy MT19937 stream
 (gen_testcases.py:76-80), solves every system with scipy's spsolve
@@ -71,7 +71,9 @@ def inputs_digest(a, b, c, d):
     return h.hexdigest()
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
+    """ref_root: the reference checkout whose scalar/test/gen_testcases.py
+    generates the fixtures."""
     test_dir = os.path.join(ref_root, "scalar", "test")
     sys.path.insert(0, test_dir)
     import gen_testcases as gen  # noqa: E402  (its import seeds the stream)
@@ -109,4 +111,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/reference")
+    main(sys.argv[1])

@@ -207,3 +207,24 @@ def test_blocking_and_stream_settings():
     tb.set_blocking(True)
     tb.set_stream(None)
     assert _lib.load().tridGetStream() in (None, 0)
+
+
+def test_no_alloc_entry_refuses_a_distributed_ctx():
+    """tridDmtsvStridedBatchNoAlloc has no distributed solve: a ctx whose
+    mpi_params were registered by tridDistInit is refused before any device
+    is touched, instead of solving only the local block."""
+    import numpy as np
+    from tridsolver_b200.distributed import DistContext
+
+    fn = _lib.load().tridDmtsvStridedBatchNoAlloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]
+    buf = np.zeros(64)
+    ptr = buf.ctypes.data
+    dims = (ctypes.c_int * 2)(8, 8)
+    with DistContext(1, rank=0, nranks=1, allgather=lambda *a: None) as dc:
+        st = fn(ctypes.addressof(dc.ctx), ptr, ptr, ptr, ptr, 2, 1, dims, dims)
+    assert st == TridStatus.INVALID_VALUE
+    assert not buf.any()

@@ -8,8 +8,10 @@ acceptable, use this variant instead: it keeps that scratch in one fixed
 16 MiB device array inside the library. This file checks, through the C ABI,
 that it gives the regular entry point's results (within the FP64 parity
 tolerance of the other GPU tests) on several calls in a row, which share and
-reuse the fixed array, and that a problem needing more scratch than the
-array holds is refused before anything runs.
+reuse the fixed array, that a problem needing more scratch than the
+array holds is refused before anything runs, that a long-path call leaves
+the device's free memory unchanged, and that zero pivots are reported
+through the pivot word kept in the fixed array.
 
 The file is named so that pytest collects it last; it passes run alone in a
 fresh process (the first call sets up the array's device address) as well as
@@ -79,3 +81,47 @@ def test_problem_beyond_the_fixed_array_is_refused():
     torch.cuda.synchronize()
     assert st == tb.TridStatus.INVALID_VALUE
     assert torch.equal(arrs[3], before), "a refused call must not touch d"
+
+
+def _call_fixed(arrs, dims, solvedim):
+    return _no_alloc_entry()(None, *(t.data_ptr() for t in arrs), len(dims), solvedim, _ints(dims),
+                             _ints(dims))
+
+
+def test_long_path_takes_no_device_memory():
+    """The property the entry point exists for: a long-path call (16 systems
+    of 100000 rows, about 7 MB of reduced rows) leaves the device's free
+    memory where it was, while the regular entry point takes its scratch
+    from the library's pool, which keeps it until released."""
+    dims = [100000, 16]
+    a, b, c, d = make_system(dims, 0, np.float64, seed=7)
+    arrs = [torch.from_numpy(v).cuda() for v in (a, b, c, d)]
+    tb.release_scratch()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert _call_fixed(arrs, dims, 0) == tb.TridStatus.SUCCESS
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free0 - free1 < (2 << 20), free0 - free1
+    st = tb.tridDmtsvStridedBatch(None, *arrs, 2, 0, dims, dims)
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    tb.release_scratch()
+    assert st == tb.TridStatus.SUCCESS
+    assert free1 - free2 >= (4 << 20), "the measurement sees the regular entry's scratch"
+
+
+@pytest.mark.parametrize("dims", [[16, 8], [100000]])
+def test_zero_pivot_reported_through_the_fixed_array(dims):
+    """A zero pivot is reported by a blocking call (the pivot word is the
+    first word of the fixed array), and the next clean call succeeds."""
+    a, b, c, d = make_system(dims, 0, np.float64, seed=3)
+    a[:] = 0.0
+    c[:] = 0.0
+    b[37] = 0.0
+    arrs = [torch.from_numpy(v).cuda() for v in (a, b, c, d)]
+    assert _call_fixed(arrs, dims, 0) == tb.TridStatus.ZERO_PIVOT
+    a, b, c, d = make_system(dims, 0, np.float64, seed=3)
+    arrs = [torch.from_numpy(v).cuda() for v in (a, b, c, d)]
+    assert _call_fixed(arrs, dims, 0) == tb.TridStatus.SUCCESS

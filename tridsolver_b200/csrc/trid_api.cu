@@ -179,7 +179,7 @@ static tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, b
 template <typename R, bool INC>
 static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b, const R *c, R *d,
                                   R *u, int ndim, int solvedim, const int *dims, const int *pads) {
-  // opts are hints (the autotuned plan is used for every value);
+  // opts are hints (choose_plan's plan is used for every value);
   // mpi_params selects the distributed solve only when registered
   const bool dist = ctx && dist_registered(ctx->mpi_params);
   BatchArgs<R> p;

@@ -45,8 +45,9 @@ static bool hybrid_supported(bool contig, int M, int T) {
   return false;
 }
 
-// Built-in table of rows per thread by system length and layout; the
-// autotuner can replace it per shape (see DESIGN.md for the measurements).
+// Built-in table of rows per thread by system length and layout, from
+// measurements on 256^3 and 512^3 grids (the strided streaming kernels set
+// their own rows per thread in choose_plan).
 template <typename R>
 static int default_m(int N, bool contig) {
   if (contig) {

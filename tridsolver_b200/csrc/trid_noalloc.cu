@@ -27,7 +27,14 @@
 //     on one device) race on the array; serialise them;
 //   * the first call on each device looks up the array's device address with
 //     that device current (cudaGetSymbolAddress) and caches it; make that
-//     first call before any stream capture.
+//     first call before any stream capture. The cached address is not looked
+//     up again, so a cudaDeviceReset after the first call (which unloads the
+//     library's device code) is not supported;
+//   * the plan is always the automatic one: tridForcePlan and the other
+//     tridForce* settings of the calling thread are ignored;
+//   * a ctx whose mpi_params were registered by tridDistInit (the distributed
+//     solve, whose exchange allocates) is refused with
+//     TRID_STATUS_INVALID_VALUE instead of solving only the local block.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -134,7 +141,13 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchNoAlloc(const TridParams *ctx, const 
                                                    const double *b, const double *c, double *d,
                                                    int ndim, int solvedim, const int *dims,
                                                    const int *pads) {
-  (void)ctx;
+  const TraceScope trace("tridDmtsvStridedBatchNoAlloc");
+  if (ctx && dist_registered(ctx->mpi_params)) {
+    fprintf(stderr,
+            "tridDmtsvStridedBatchNoAlloc: ctx->mpi_params selects the distributed solve, which this "
+            "entry point does not provide (use tridDmtsvStridedBatch)\n");
+    return TRID_STATUS_INVALID_VALUE;
+  }
   BatchArgs<double> p;
   bool empty = false;
   tridStatus_t st = describe_batch(a, b, c, d, ndim, solvedim, dims, pads, &p, &empty);

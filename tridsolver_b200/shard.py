@@ -8,11 +8,12 @@ pads) problem shape the C ABI takes, so no data moves between ranks. This is
 "weak scaling" when every rank holds its own grid, as bench.py runs it, and
 "strong scaling" when ranks split one grid.
 
-A z-slab decomposition of a full ADI step (x and y local, z across ranks)
-would need the reference's partition method across GPUs. That method is
-`scalar/src/cuda/trid_cuda_mpi.cu:218-605`: an allgather of 6 values per
-system boundary, then a reduced solve. It is not part of this single-GPU
-library.
+Systems that themselves span ranks (a z-slab decomposition of a full ADI
+step: x and y local, z across ranks) need an exchange instead: the
+partition method of the reference's MPI/NCCL build
+(`scalar/src/cuda/trid_cuda_mpi.cu:218-605`), an all-gather of 6 values per
+system and rank, then a reduced solve. That is `tridsolver_b200.distributed`
+(the library's distributed solve behind ctx->mpi_params), not this module.
 """
 
 
