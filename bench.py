@@ -475,10 +475,17 @@ def config_adi(dev, hbm, n=(256, 256, 256), steps=100, dtype="f64", alpha=1.0):
 
 
 def config_precision(dev, n=512, dims=None):
-    """FP32 storage + FP32 solve with on-chip FP64 refinement vs the plain FP64
-    solve, along x and z, margins log-uniform [10^lo, 1]. For strided axes the
-    library's automatic choice is the direct FP64 solve of the FP32 values;
-    both it and the refinement (forced, so its passes are reported) are timed."""
+    """FP64-specified systems (margins b - |a| - |c| log-uniform in [10^lo, 1])
+    solved along x and z three ways, each timed and its error measured
+    against the direct FP64 solve of the FP64 system (tridDmtsvStridedBatch,
+    which the GPU tests pin to the reference CPU solver at 1e-12):
+      * refine_fp64_system: tridDmtsvStridedBatchRefine, the FP32
+        factorisation of the rounded coefficients refined with the FP64
+        residual of the FP64 system (40 bytes per element, one pass);
+      * fp32_values: tridDmtsvStridedBatchMixed on the coefficients rounded
+        to FP32, which solves that rounded system exactly (28 bytes per
+        element); its error against the FP64 system is the rounding's;
+      * fp64_ms: the direct FP64 solve itself."""
     import torch
     import tridsolver_b200 as tb
     stream = torch.cuda.current_stream()
@@ -486,43 +493,52 @@ def config_precision(dev, n=512, dims=None):
     shape = tuple(reversed(dims))
     out = []
 
-    def mixed(a32, b32, c32, x, axis):
-        return tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, x, 3, axis, dims, dims, 12, 1e-12)
+    def rel(x, ref):
+        return ((x - ref).abs().max() / ref.abs().max()).item()
 
     for lo in (-3, -2, -1, 0):
         a, b, c, d = _system(shape, torch.float64, dev, 7 - lo, margin_lo=lo if lo < 0 else None)
         a32, b32, c32 = a.float(), b.float(), c.float()
-        del a, b, c
-        a64, b64, c64 = a32.double(), b32.double(), c32.double()
         for axis in (0, 2):
-            x64 = d.clone()
             tb.set_blocking(True)
-            tb.tridDmtsvStridedBatch(None, a64, b64, c64, x64, 3, axis, dims, dims)
-            tb.set_mixed_mode(1)  # the refinement, so its passes are reported
+            x64 = d.clone()
+            tb.tridDmtsvStridedBatch(None, a, b, c, x64, 3, axis, dims, dims)
+            xr = d.clone()
+            st_r, it_r, est_r = tb.tridDmtsvStridedBatchRefine(None, a, b, c, xr, 3, axis, dims, dims,
+                                                               12, 1e-12)
+            err_r = rel(xr, x64)
+            xp = d.clone()
+            tb.tridDmtsvStridedBatch(None, a32.double(), b32.double(), c32.double(), xp, 3, axis,
+                                     dims, dims)
             xm = d.clone()
-            st, iters, corr = mixed(a32, b32, c32, xm, axis)
-            err = ((xm - x64).abs().max() / x64.abs().max()).item()
-            tb.set_mixed_mode(0)
-            xa = d.clone()
-            st_a, iters_a, _ = mixed(a32, b32, c32, xa, axis)
-            err_a = ((xa - x64).abs().max() / x64.abs().max()).item()
+            st_m, it_m, _ = tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, xm, 3, axis, dims,
+                                                          dims, 12, 1e-12)
+            err_m_own, err_m_64 = rel(xm, xp), rel(xm, x64)
             tb.set_blocking(False)
             w = d.clone()
-            t64 = _timed(lambda: tb.tridDmtsvStridedBatch(None, a64, b64, c64, w, 3, axis, dims, dims),
-                         5, stream)
-            tb.set_mixed_mode(1)
-            tref = _timed(lambda: mixed(a32, b32, c32, w, axis), 5, stream)
-            tb.set_mixed_mode(0)
-            tauto = _timed(lambda: mixed(a32, b32, c32, w, axis), 5, stream)
-            out.append({"margin_min": 10.0 ** lo, "axis": "xyz"[axis], "status": st,
-                        "iterations": iters, "final_rel_correction": corr,
-                        "max_rel_error_vs_fp64": err, "fp64_ms": round(t64, 4),
-                        "refine_ms": round(tref, 4),
-                        "mixed_ms": round(tauto, 4), "mixed_over_fp64_time": round(tauto / t64, 3),
-                        "mixed_strategy": "refinement" if iters_a else "direct FP64 solve of the FP32 values",
-                        "mixed_status": st_a, "mixed_error_vs_fp64": err_a})
-            del x64, xm, xa, w
-        del a32, b32, c32, a64, b64, c64, d
+            t64 = _timed(lambda: tb.tridDmtsvStridedBatch(None, a, b, c, w, 3, axis, dims, dims), 5,
+                         stream)
+            tr = _timed(lambda: tb.tridDmtsvStridedBatchRefine(None, a, b, c, w, 3, axis, dims, dims,
+                                                               12, 1e-12), 5, stream)
+            tm = _timed(lambda: tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, w, 3, axis, dims,
+                                                              dims, 12, 1e-12), 5, stream)
+            tb.set_blocking(True)
+            out.append({
+                "margin_min": 10.0 ** lo, "axis": "xyz"[axis], "fp64_ms": round(t64, 4),
+                "refine_fp64_system": {
+                    "status": st_r, "iterations": it_r, "estimated_rel_error": est_r,
+                    "max_rel_error_vs_fp64_system": err_r, "ms": round(tr, 4),
+                    "time_over_fp64": round(tr / t64, 3), "bytes_per_element": 40,
+                    "reaches_1e-12": err_r <= 1e-12},
+                "fp32_values": {
+                    "status": st_m, "iterations": it_m,
+                    "strategy": "refinement" if it_m else "direct FP64 solve of the FP32 values",
+                    "max_rel_error_vs_fp64_of_fp32_values": err_m_own,
+                    "max_rel_error_vs_fp64_system": err_m_64, "ms": round(tm, 4),
+                    "time_over_fp64": round(tm / t64, 3), "bytes_per_element": 28},
+            })
+            del x64, xr, xp, xm, w
+        del a32, b32, c32, a, b, c, d
         torch.cuda.empty_cache()
     return out
 

@@ -266,6 +266,30 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
                                                  const int *pads, int max_iters, double tol,
                                                  int *iters_out, double *correction_out);
 
+/* ---- FP32 factorisation, FP64-specified system ----------------------------
+ * No counterpart in the reference. Solves T x = d for an FP64-specified
+ * system (a, b, c, d FP64 arrays; x overwrites d) by iterative refinement:
+ * the FP32 factorisation of the coefficients rounded to FP32 is computed
+ * once, on chip, and every pass forms the residual r = d - T x in FP64 with
+ * the FP64 coefficients, solves T dx = r with the FP32 factors and
+ * accumulates x += dx in FP64, until the estimated relative error (the
+ * contraction estimate of tridDmtsvStridedBatchMixed) is at most tol for
+ * every system, or max_iters FP32 solves. The result converges to the
+ * solution of the FP64 system itself (tridDmtsvStridedBatchMixed instead
+ * solves the system of its FP32 values exactly). One pass over memory: a, b,
+ * c, d read once and x written once, 40 bytes per element, the same as
+ * tridDmtsvStridedBatch, so it is not faster than the direct FP64 solve; it
+ * exists for callers that want the FP32 factorisation with an FP64 error
+ * bound and iteration count per call. Blocking calls report the largest
+ * iteration count and error estimate in *iters_out / *correction_out (-1
+ * when not blocking). N <= 512 (longer systems return
+ * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
+EXTERN_C tridStatus_t tridDmtsvStridedBatchRefine(const TridParams *ctx, const double *a,
+                                                  const double *b, const double *c, double *d,
+                                                  int ndim, int solvedim, const int *dims,
+                                                  const int *pads, int max_iters, double tol,
+                                                  int *iters_out, double *correction_out);
+
 /* ---- solve without allocating ------------------------------------------
  * No counterpart in the reference. tridDmtsvStridedBatch with the same
  * arguments and results, for callers that cannot allocate device memory

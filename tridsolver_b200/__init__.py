@@ -13,5 +13,6 @@ from .api import (  # noqa: F401
     set_mixed_mode,
     set_blocking, set_stream, solve, solve_batched_trid, strided_batch, tridDmtsvStridedBatch,
     tridDmtsvStridedBatchAdjoint, tridDmtsvStridedBatchInc, tridDmtsvStridedBatchMixed,
+    tridDmtsvStridedBatchRefine,
     tridSmtsvStridedBatch, tridSmtsvStridedBatchAdjoint, tridSmtsvStridedBatchInc)
 from ._lib import LIB_PATH, load as load_library  # noqa: F401

@@ -51,6 +51,8 @@ SYMBOLS = {
     "tridSmtsvStridedBatchAdjoint": (_I, [_P] * 10 + [_I, _I, _IP, _IP]),
     "tridDmtsvStridedBatchMixed": (_I, [_P, _P, _P, _P, _P, _I, _I, _IP, _IP, _I, ctypes.c_double,
                                         _IP, ctypes.POINTER(ctypes.c_double)]),
+    "tridDmtsvStridedBatchRefine": (_I, [_P, _P, _P, _P, _P, _I, _I, _IP, _IP, _I, ctypes.c_double,
+                                        _IP, ctypes.POINTER(ctypes.c_double)]),
     "tridSetMixedMode": (_I, [_I]),
     "tridDistInit": (_I, [_P, _I, _I, _I, _P, _P]),
     "tridDistFinalize": (_I, [_P]),

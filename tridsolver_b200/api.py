@@ -127,6 +127,21 @@ def tridDmtsvStridedBatchMixed(ctx, a, b, c, d, ndim, solvedim, dims, pads, max_
     return st, it.value, corr.value
 
 
+def tridDmtsvStridedBatchRefine(ctx, a, b, c, d, ndim, solvedim, dims, pads, max_iters=10,
+                                tol=1e-12):
+    """FP64-specified a, b, c, d (x overwrites d): FP32 factorisation of the
+    rounded coefficients, refined with the FP64 residual of the FP64 system
+    on chip (include/tridsolver_b200.h). Returns (status, iterations,
+    estimated relative error); the last two are -1 unless blocking."""
+    it = ctypes.c_int(-1)
+    corr = ctypes.c_double(-1.0)
+    st = _lib.load().tridDmtsvStridedBatchRefine(_ctx(ctx), _addr(a), _addr(b), _addr(c), _addr(d),
+                                                 int(ndim), int(solvedim), _ints(dims),
+                                                 _ints(pads), int(max_iters), float(tol),
+                                                 ctypes.byref(it), ctypes.byref(corr))
+    return st, it.value, corr.value
+
+
 def tridDmtsvStridedBatchAdjoint(ctx, a, b, c, x, w, dbar, abar, bbar, cbar, ndim, solvedim, dims,
                                  pads):
     """Adjoint of the strided solve (include/tridsolver_b200.h); abar, bbar,

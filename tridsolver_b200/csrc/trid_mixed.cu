@@ -1,18 +1,24 @@
-// FP32-storage / FP32-solve tridiagonal batch with FP64 iterative refinement.
+// FP32-solve tridiagonal batch with FP64 iterative refinement, in two forms:
 //
-// Solves T x = d where the coefficients a, b, c are stored in FP32 (and taken
-// exactly, promoted to FP64, as the system to solve) and d, x are FP64:
+//  * tridDmtsvStridedBatchMixed: the coefficients a, b, c are stored in FP32
+//    and taken exactly, promoted to FP64, as the system to solve;
+//  * tridDmtsvStridedBatchRefine: the system is specified in FP64 (a, b, c
+//    are FP64 arrays); the FP32 factorisation is formed from their rounded
+//    values, and the residual uses the FP64 values, so refinement converges
+//    to the solution of the FP64 system itself.
+//
+// In both, d and x are FP64:
 //
 //   x = 0;  repeat:  r = d - T x       (FP64: FP32 coefficients times FP64 x)
 //                    solve T dx = r    (FP32: the partition hybrid)
 //                    x += dx           (FP64)
 //   until max|dx| <= tol * max|x| over the system, or max_iters solves.
 //
-// Everything after the one read of a, b, c, d happens on chip: the FP32
+// Everything after the one read of a, b, c, d happens on chip: the
 // coefficients stay in shared memory (contiguous systems) or registers
-// (strided), d and x in registers, and x is written once. A pass moves
-// 3*4 + 8 + 8 = 28 bytes per element against 40 for the plain FP64 solve, so
-// refinement to FP64 accuracy can cost less time than the FP64 solve.
+// (strided), d and x in registers, and x is written once. With FP32
+// coefficients a call moves 3*4 + 8 + 8 = 28 bytes per element against 40
+// for the plain FP64 solve; with FP64 coefficients it moves the same 40.
 // The reference has no mixed-precision entry point; this is an extension
 // (include/tridsolver_b200.h).
 #include <cuda_runtime.h>
@@ -24,8 +30,10 @@
 
 namespace trid {
 
-struct MixedArgs {
-  const float *a, *b, *c;
+// CT: the coefficients' storage type (float: the FP32 values are the system;
+// double: the FP64 values are, and only the factorisation is rounded).
+template <typename CT> struct MixedArgsT {
+  const CT *a, *b, *c;
   double *d;  // right-hand side in, x out
   int N;
   long long nsys, n0, st0, st1, stride;
@@ -33,6 +41,7 @@ struct MixedArgs {
   double tol;
   unsigned *flag;
 };
+using MixedArgs = MixedArgsT<float>;
 
 // Per-call statistics: the largest iteration count and the largest final
 // relative correction max|dx|/max|x| over all systems (as ordered bits; both
@@ -70,7 +79,8 @@ __device__ __forceinline__ double mixed_error_estimate(float dmax, float dprev, 
   return est / xmax;
 }
 
-__device__ __forceinline__ long long mixed_base(const MixedArgs &p, long long s) {
+template <typename CT>
+__device__ __forceinline__ long long mixed_base(const MixedArgsT<CT> &p, long long s) {
   const long long i1 = s / p.n0;
   return (s - i1 * p.n0) * p.st0 + i1 * p.st1;
 }
@@ -153,12 +163,53 @@ __device__ __forceinline__ void fp32_chunk_solve(float (&wa)[M], float (&wb)[M],
   chunk_substitute<float, M>(wa, wc, wd, y, z);
 }
 
+// Four rows (4q .. 4q+3) of a swizzled coefficient tile as FP64.
+template <typename CT, int M>
+__device__ __forceinline__ void lds4_swz(const CT *tile, int l, int q, double (&v)[4]) {
+  using S = Swz<CT, M>;
+  if constexpr (sizeof(CT) == 4) {
+    const float4 x = *reinterpret_cast<const float4 *>(tile + S::unit(l, q));
+    v[0] = x.x;
+    v[1] = x.y;
+    v[2] = x.z;
+    v[3] = x.w;
+  } else {
+    const double2 x = *reinterpret_cast<const double2 *>(tile + S::unit(l, 2 * q));
+    const double2 y = *reinterpret_cast<const double2 *>(tile + S::unit(l, 2 * q + 1));
+    v[0] = x.x;
+    v[1] = x.y;
+    v[2] = y.x;
+    v[3] = y.y;
+  }
+}
+
+// A lane's coefficient row from its tile with the fix-ups of the first pass
+// (identity rows past the end, a[0] = 0, c[N-1] = 0: kind 0 = a, 1 = b,
+// 2 = c) written back when the chunk needs them, rounded to FP32.
+template <typename CT, int M>
+__device__ __forceinline__ void load_fixed_row(CT *tile, int lane, int row0, int N, int kind,
+                                               float (&w)[M]) {
+  CT v[M];
+  lds_swz<CT, M>(tile, lane, v);
+  if (row0 == 0 || row0 + M >= N) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      const int row = row0 + i;
+      if (row >= N) v[i] = kind == 1 ? CT(1) : CT(0);
+      if (kind == 0 && row == 0) v[i] = CT(0);
+      if (kind == 2 && row == N - 1) v[i] = CT(0);
+    }
+    sts_swz<CT, M>(tile, lane, v);
+  }
+#pragma unroll
+  for (int i = 0; i < M; ++i) w[i] = (float)v[i];
+}
+
 // ---------------------------------------------------------------------------
 // Contiguous systems (stride 1), one warp per system, 16-byte aligned starts.
-// The warp stages a, b, c (FP32) and d (FP64) through shared memory with
-// coalesced 16-byte cp.async copies into padded rows (one spare 16-byte unit
-// per chunk row, so a lane's 16-byte reads of its own row are conflict-free),
-// as contig_smem_kernel does.
+// The warp stages a, b, c (as stored: FP32 or FP64) and d (FP64) through
+// shared memory with coalesced 16-byte cp.async copies into swizzled,
+// unpadded rows (a lane's 16-byte reads of its own row are conflict-free).
 //
 // The FP32 solve is factored once: the first pass records, per row, the
 // pivot reciprocal r and the forward-eliminated a' (shared memory, next to
@@ -170,22 +221,26 @@ __device__ __forceinline__ void fp32_chunk_solve(float (&wa)[M], float (&wb)[M],
 //   reduced   de <- (de - al_l de_left - ga_l de_right) r_l per PCR level
 //   back-substitution  dx_i = d'_i - a'_i dx_first - c'_i dx_{i+1}
 // which is a few FP32 operations per row instead of a fresh elimination.
-template <int M>
-__global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p) {
+// The residual uses the coefficients as stored (exactly, in FP64).
+template <int M, typename CT>
+__global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgsT<CT> p) {
   static_assert(M % 4 == 0 && M >= 8, "rows per lane");
+  using SC = Swz<CT, M>;
   using SF = Swz<float, M>;
   using SD = Swz<double, M>;
-  constexpr int BF = 32 * M;    // floats per FP32 tile
-  constexpr int BD = 32 * M;    // doubles per FP64 tile
-  constexpr int NT = 5;         // FP32 tiles: a, b, c (fixed), r, a' (c' = r c is recomputed)
+  constexpr int BF = 32 * M;    // elements per tile
+  constexpr int VC = 16 / (int)sizeof(CT);  // coefficients per 16-byte unit
+  // tiles: a, b, c (as stored, fixed), then FP32 r and a' (c' = r c is
+  // recomputed), then FP64 d
+  constexpr int PER_WARP = 3 * BF * (int)sizeof(CT) + 2 * BF * 4 + BF * 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char *wbase = smem_raw + (threadIdx.x >> 5) * (NT * BF * 4 + BD * 8);
-  float *ta = reinterpret_cast<float *>(wbase);
-  float *tb = ta + BF;
-  float *tc = tb + BF;
-  float *tr = tc + BF;
+  unsigned char *wbase = smem_raw + (threadIdx.x >> 5) * PER_WARP;
+  CT *ta = reinterpret_cast<CT *>(wbase);
+  CT *tb = ta + BF;
+  CT *tc = tb + BF;
+  float *tr = reinterpret_cast<float *>(tc + BF);
   float *tfa = tr + BF;
-  double *td = reinterpret_cast<double *>(wbase + NT * BF * 4);
+  double *td = reinterpret_cast<double *>(tfa + BF);
   const int lane = threadIdx.x & 31;
   const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (s >= p.nsys) return;  // uniform per warp
@@ -194,9 +249,9 @@ __global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p)
   const bool full = N == 32 * M;  // every lane's chunk full: unrolled copies
   if (full) {
 #pragma unroll
-    for (int k = 0; k < M / 4; ++k) {
-      const int e = 4 * (lane + 32 * k);
-      const int o = SF::off(e);
+    for (int k = 0; k < M / VC; ++k) {
+      const int e = VC * (lane + 32 * k);
+      const int o = SC::off(e);
       cp_async16(ta + o, p.a + base + e, 16);
       cp_async16(tb + o, p.b + base + e, 16);
       cp_async16(tc + o, p.c + base + e, 16);
@@ -207,11 +262,11 @@ __global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p)
       cp_async16(td + SD::off(e), p.d + base + e, 16);
     }
   } else {
-    const int nu = (N + 3) / 4;  // FP32 units of 4
+    const int nu = (N + VC - 1) / VC;  // coefficient units
     for (int un = lane; un < nu; un += 32) {
-      const int e = un * 4;
-      const int left = (N - e) >= 4 ? 16 : (N - e) * 4;
-      const int o = SF::off(e);
+      const int e = un * VC;
+      const int left = (N - e) >= VC ? 16 : (N - e) * (int)sizeof(CT);
+      const int o = SC::off(e);
       cp_async16(ta + o, p.a + base + e, left);
       cp_async16(tb + o, p.b + base + e, left);
       cp_async16(tc + o, p.c + base + e, left);
@@ -231,27 +286,15 @@ __global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p)
   // ---- first pass: fix the coefficients (identity rows past the end, a[0]
   // and c[N-1] zero), factor, and solve T x = (float)d
   float wa[M], wb[M], wc[M], wd[M];
-  lds_swz<float, M>(ta, lane, wa);
-  lds_swz<float, M>(tb, lane, wb);
-  lds_swz<float, M>(tc, lane, wc);
+  load_fixed_row<CT, M>(ta, lane, row0, N, 0, wa);
+  load_fixed_row<CT, M>(tb, lane, row0, N, 1, wb);
+  load_fixed_row<CT, M>(tc, lane, row0, N, 2, wc);
   double dd[M];
   lds_swz<double, M>(td, lane, dd);
-  if (row0 == 0 || row0 + M >= N) {  // chunks holding row 0, row N-1 or rows past the end
+  if (row0 + M >= N) {  // chunks holding rows past the end
 #pragma unroll
-    for (int i = 0; i < M; ++i) {
-      const int row = row0 + i;
-      if (row >= N) {
-        wa[i] = 0.f;
-        wb[i] = 1.f;
-        wc[i] = 0.f;
-        dd[i] = 0.0;
-      }
-      if (row == 0) wa[i] = 0.f;
-      if (row == N - 1) wc[i] = 0.f;
-    }
-    sts_swz<float, M>(ta, lane, wa);
-    sts_swz<float, M>(tb, lane, wb);
-    sts_swz<float, M>(tc, lane, wc);
+    for (int i = 0; i < M; ++i)
+      if (row0 + i >= N) dd[i] = 0.0;
     sts_swz<double, M>(td, lane, dd);
   }
 #pragma unroll
@@ -397,33 +440,39 @@ __global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p)
     if (lane == 31) xr = 0.0;
 #pragma unroll
     for (int q = 0; q < M / 4; ++q) {
-      const float4 a4 = *reinterpret_cast<const float4 *>(ta + SF::unit(lane, q));
-      const float4 b4 = *reinterpret_cast<const float4 *>(tb + SF::unit(lane, q));
-      const float4 c4 = *reinterpret_cast<const float4 *>(tc + SF::unit(lane, q));
+      double av[4], bv[4], cv[4];
+      lds4_swz<CT, M>(ta, lane, q, av);
+      lds4_swz<CT, M>(tb, lane, q, bv);
+      lds4_swz<CT, M>(tc, lane, q, cv);
       const float4 r4 = *reinterpret_cast<const float4 *>(tr + SF::unit(lane, q));
       const double2 d01 = *reinterpret_cast<const double2 *>(td + SD::unit(lane, 2 * q));
       const double2 d23 = *reinterpret_cast<const double2 *>(td + SD::unit(lane, 2 * q + 1));
-      const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
-      const float cv[4] = {c4.x, c4.y, c4.z, c4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+      const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
       const double dv[4] = {d01.x, d01.y, d23.x, d23.y};
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int i = 4 * q + k;
         const double xm = i == 0 ? xl : x64[i - 1];
         const double xp = i == M - 1 ? xr : x64[i + 1];
-        double res = dv[k] - (double)bv[k] * x64[i];
-        res = fma(-(double)av[k], xm, res);
-        res = fma(-(double)cv[k], xp, res);
+        // FP64 residual with the coefficients as stored
+        double res = dv[k] - bv[k] * x64[i];
+        res = fma(-av[k], xm, res);
+        res = fma(-cv[k], xp, res);
         const float rf = (float)res;
-        wd[i] = i < 2 ? rv[k] * rf : rv[k] * (rf - av[k] * wd[i - 1]);
+        // the factorisation's FP32 a
+        const float af = (float)av[k];
+        wd[i] = i < 2 ? rv[k] * rf : rv[k] * (rf - af * wd[i - 1]);
       }
     }
     float fa[M], fc[M], rr2[M];
     lds_swz<float, M>(tfa, lane, fa);
     lds_swz<float, M>(tr, lane, rr2);
-    lds_swz<float, M>(tc, lane, fc);
+    {
+      CT cs[M];
+      lds_swz<CT, M>(tc, lane, cs);
 #pragma unroll
-    for (int j = 0; j < M; ++j) fc[j] *= rr2[j];
+      for (int j = 0; j < M; ++j) fc[j] = (float)cs[j] * rr2[j];
+    }
     float D2 = wd[M - 2];
 #pragma unroll
     for (int j = M - 3; j >= 1; --j) D2 = wd[j] - fc[j] * D2;
@@ -467,9 +516,9 @@ __global__ void __launch_bounds__(32, 14) mixed_contig_kernel(const MixedArgs p)
 // through shared memory for the residual, and every FP32 solve uses the
 // block-level reduced solve. The block iterates until all its systems have
 // converged (or max_iters), so the loop is uniform across the block.
-template <int M, int KR>
+template <int M, int KR, typename CT>
 __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
-    mixed_strided_kernel(const MixedArgs p, int T, int W, long long ngx) {
+    mixed_strided_kernel(const MixedArgsT<CT> p, int T, int W, long long ngx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int TW = T * W;
   double *xf = reinterpret_cast<double *>(smem_raw);  // first x of chunk (t, s)
@@ -490,21 +539,21 @@ __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
   const long long base = i0 * p.st0 + i1 * p.st1;
   const int N = p.N;
   const int row0 = t * M;
-  float ra[M], rb[M], rc[M];
+  CT ra[M], rb[M], rc[M];  // the coefficients as stored
   double d64[M], x64[M];
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const int row = row0 + i;
     if (active && row < N) {
       const long long o = base + (long long)row * p.stride;
-      ra[i] = row == 0 ? 0.f : __ldg(p.a + o);
+      ra[i] = row == 0 ? CT(0) : __ldg(p.a + o);
       rb[i] = __ldg(p.b + o);
-      rc[i] = row == N - 1 ? 0.f : __ldg(p.c + o);
+      rc[i] = row == N - 1 ? CT(0) : __ldg(p.c + o);
       d64[i] = p.d[o];
     } else {
-      ra[i] = 0.f;
-      rb[i] = 1.f;
-      rc[i] = 0.f;
+      ra[i] = CT(0);
+      rb[i] = CT(1);
+      rc[i] = CT(0);
       d64[i] = 0.0;
     }
     x64[i] = 0.0;
@@ -516,9 +565,9 @@ __global__ void __launch_bounds__(KR >= 4 ? 512 : 256)
     float wa[M], wb[M], wc[M], wd[M];
 #pragma unroll
     for (int i = 0; i < M; ++i) {
-      wa[i] = ra[i];
-      wb[i] = rb[i];
-      wc[i] = rc[i];
+      wa[i] = (float)ra[i];
+      wb[i] = (float)rb[i];
+      wc[i] = (float)rc[i];
     }
     if (it == 0) {
 #pragma unroll
@@ -703,45 +752,58 @@ static int pow2c(long long v) {
   return q;
 }
 
-// One warp per CTA: ~20 KB of shared memory per system, so up to 11 warps
-// per SM; larger CTAs would round the shared-memory use up.
-template <int M>
-static cudaError_t launch_mixed_contig(const MixedArgs &p, cudaStream_t st) {
+// One warp per CTA: 14 KB (FP32 coefficients) or 20 KB (FP64) of shared
+// memory per system of up to 512 rows, so up to 14 or 11 warps per SM;
+// larger CTAs would round the shared-memory use up.
+template <int M, typename CT>
+static cudaError_t launch_mixed_contig(const MixedArgsT<CT> &p, cudaStream_t st) {
   const int threads = 32;
-  const size_t per_warp = (size_t)5 * 32 * M * 4 + (size_t)32 * M * 8;
+  const size_t per_warp = (size_t)3 * 32 * M * sizeof(CT) + (size_t)2 * 32 * M * 4 + (size_t)32 * M * 8;
   const size_t smem = per_warp * (threads / 32);
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(mixed_contig_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(mixed_contig_kernel<M, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long blocks = (p.nsys * 32 + threads - 1) / threads;
-  mixed_contig_kernel<M><<<(unsigned)blocks, threads, smem, st>>>(p);
+  mixed_contig_kernel<M, CT><<<(unsigned)blocks, threads, smem, st>>>(p);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 
-template <int M, int KR>
-static cudaError_t launch_mixed_strided(const MixedArgs &p, int T, int W, cudaStream_t st) {
+template <int M, int KR, typename CT>
+static cudaError_t launch_mixed_strided(const MixedArgsT<CT> &p, int T, int W, cudaStream_t st) {
   const long long ngx = (p.n0 + W - 1) / W;
   const long long blocks = ngx * (p.nsys / p.n0);
   const size_t smem = (size_t)(4 * T * W + 2 * W) * 8 + (size_t)(W + (W & 1)) * 4 +
                       (size_t)6 * T * (W + 1) * 4;
-  mixed_strided_kernel<M, KR><<<(unsigned)blocks, W * T, smem, st>>>(p, T, W, ngx);
+  mixed_strided_kernel<M, KR, CT><<<(unsigned)blocks, W * T, smem, st>>>(p, T, W, ngx);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 
-}  // namespace trid
+// The refinement kernels for any layout: staged contiguous systems of
+// 129..512 rows, the generic strided form otherwise (N <= 512).
+template <typename CT>
+static cudaError_t launch_refinement(const MixedArgsT<CT> &p, cudaStream_t st) {
+  const int N = p.N;
+  auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+  const long long unit = 16 / (long long)sizeof(CT);
+  const bool staged = p.stride == 1 && al(p.a) && al(p.b) && al(p.c) && al(p.d) &&
+                      p.st0 % unit == 0 && p.st1 % unit == 0 && p.st0 % 2 == 0 &&
+                      p.st1 % 2 == 0 && N > 128;
+  if (staged) return N <= 256 ? launch_mixed_contig<8, CT>(p, st) : launch_mixed_contig<16, CT>(p, st);
+  // generic addressing (strided, or contiguous but unaligned or short)
+  const int T = pow2c((N + 7) / 8);
+  int W = 512 / T > 16 ? 16 : 512 / T;
+  if (T <= 32 && W * T > 256) W = 256 / T;
+  if (W * T < 32) W = 32 / T;
+  if (T <= 32) return launch_mixed_strided<8, 2, CT>(p, T, W, st);
+  return launch_mixed_strided<8, 4, CT>(p, T, W, st);
+}
 
-using namespace trid;
-
-EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const float *a,
-                                                 const float *b, const float *c, double *d,
-                                                 int ndim, int solvedim, const int *dims_p,
-                                                 const int *pads_p, int max_iters, double tol,
-                                                 int *iters_out, double *correction_out) {
-  const TraceScope trace("tridDmtsvStridedBatchMixed");
-  (void)ctx;
-  if (iters_out) *iters_out = -1;
-  if (correction_out) *correction_out = -1.0;
+// Argument checks and the batch description shared by the two entry points.
+template <typename CT>
+static tridStatus_t make_mixed_args(const CT *a, const CT *b, const CT *c, double *d, int ndim,
+                                    int solvedim, const int *dims_p, const int *pads_p,
+                                    int max_iters, double tol, MixedArgsT<CT> *out, bool *empty) {
   if (ndim < 1 || ndim > MAXDIM || solvedim < 0 || solvedim >= ndim || !dims_p || !pads_p ||
       max_iters < 1 || !(tol >= 0.0))
     return TRID_STATUS_INVALID_VALUE;
@@ -752,13 +814,10 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
     pads[i] = pads_p[i];
     if (i < ndim - 1 && pads[i] < dims[i]) return TRID_STATUS_INVALID_VALUE;
   }
-  if (dims[0] * dims[1] * dims[2] == 0) {
-    if (iters_out) *iters_out = 0;
-    if (correction_out) *correction_out = 0.0;
-    return TRID_STATUS_SUCCESS;
-  }
+  *empty = dims[0] * dims[1] * dims[2] == 0;
+  if (*empty) return TRID_STATUS_SUCCESS;
   if (!a || !b || !c || !d) return TRID_STATUS_INVALID_VALUE;
-  MixedArgs p{};
+  MixedArgsT<CT> p{};
   p.a = a;
   p.b = b;
   p.c = c;
@@ -786,13 +845,62 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
     p.st1 = pads[0];
     p.stride = s01;
   }
+  *out = p;
+  return TRID_STATUS_SUCCESS;
+}
+
+static tridStatus_t device_ready() {
   int dev = 0, major = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
     cudaGetLastError();
     return TRID_STATUS_NOT_INITIALIZED;
   }
-  if (major != 10) return TRID_STATUS_ARCH_MISMATCH;
+  return major == 10 ? TRID_STATUS_SUCCESS : TRID_STATUS_ARCH_MISMATCH;
+}
+
+// Waits for a blocking refinement call and reports its statistics.
+static tridStatus_t finish_refinement(const Settings &cfg, int *iters_out, double *correction_out) {
+  cudaError_t e = cudaStreamSynchronize(cfg.stream);
+  if (e != cudaSuccess) return status_of(e);
+  MixedStats st{};
+  e = cudaMemcpyFromSymbol(&st, g_mixed_stats, sizeof(st));
+  if (e != cudaSuccess) return status_of(e);
+  if (iters_out) *iters_out = (int)st.iters;
+  if (correction_out) {
+    double v;
+    memcpy(&v, &st.corr_bits, sizeof(v));
+    *correction_out = v;
+  }
+  if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+  return TRID_STATUS_SUCCESS;
+}
+
+}  // namespace trid
+
+using namespace trid;
+
+EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const float *a,
+                                                 const float *b, const float *c, double *d,
+                                                 int ndim, int solvedim, const int *dims_p,
+                                                 const int *pads_p, int max_iters, double tol,
+                                                 int *iters_out, double *correction_out) {
+  const TraceScope trace("tridDmtsvStridedBatchMixed");
+  (void)ctx;
+  if (iters_out) *iters_out = -1;
+  if (correction_out) *correction_out = -1.0;
+  MixedArgs p{};
+  bool empty = false;
+  tridStatus_t sts = make_mixed_args<float>(a, b, c, d, ndim, solvedim, dims_p, pads_p, max_iters,
+                                            tol, &p, &empty);
+  if (sts != TRID_STATUS_SUCCESS) return sts;
+  if (empty) {
+    if (iters_out) *iters_out = 0;
+    if (correction_out) *correction_out = 0.0;
+    return TRID_STATUS_SUCCESS;
+  }
+  sts = device_ready();
+  if (sts != TRID_STATUS_SUCCESS) return sts;
   const Settings &cfg = settings();
   p.flag = pivot_flag_device();
   if (cfg.blocking) pivot_flag_take();
@@ -800,10 +908,15 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
   cudaError_t e = cudaMemcpyToSymbolAsync(g_mixed_stats, &zero, sizeof(zero), 0,
                                           cudaMemcpyHostToDevice, cfg.stream);
   const int N = p.N;
+  if (N > 512) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
   // strided batches the streaming kernel covers: the promoted solve (FP64
   // arithmetic on the FP32 values) unless refinement is asked for
   const bool can_promote = p.stride != 1 && N > 64 && N <= 512;
   const bool promoted = can_promote && cfg.mixed_mode != 1;
+  auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+  const bool staged = p.stride == 1 && al(a) && al(b) && al(c) && al(d) && p.st0 % 4 == 0 &&
+                      p.st1 % 4 == 0 && N > 128;
+  const bool direct = promoted || (staged && cfg.mixed_mode != 1);
   if (e == cudaSuccess && promoted) {
     BatchArgs<double> q{};
     q.d_in = d;
@@ -820,63 +933,55 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
         : N <= 256 ? launch_strided_stream_promoted<8>(q, cf, cfg.stream)
                    : launch_strided_stream_promoted<16>(q, cf, cfg.stream);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (e != cudaSuccess) return status_of(e);
-    if (cfg.blocking) {
-      e = cudaStreamSynchronize(cfg.stream);
-      if (e != cudaSuccess) return status_of(e);
-      if (iters_out) *iters_out = 0;
-      if (correction_out) *correction_out = 0.0;
-      if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
-    }
-    return TRID_STATUS_SUCCESS;
-  }
-  if (e == cudaSuccess) {
-    auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
-    const bool staged = p.stride == 1 && al(a) && al(b) && al(c) && al(d) && p.st0 % 4 == 0 &&
-                        p.st1 % 4 == 0 && N > 128;
-    if (N > 512) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
-    if (staged && cfg.mixed_mode != 1) {
-      // direct FP64 solve of the promoted values
-      e = N <= 256 ? launch_contig_promoted<8>(p, cfg.stream) : launch_contig_promoted<16>(p, cfg.stream);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      if (e != cudaSuccess) return status_of(e);
-      if (cfg.blocking) {
-        e = cudaStreamSynchronize(cfg.stream);
-        if (e != cudaSuccess) return status_of(e);
-        if (iters_out) *iters_out = 0;
-        if (correction_out) *correction_out = 0.0;
-        if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
-      }
-      return TRID_STATUS_SUCCESS;
-    }
-    if (staged) {
-      e = N <= 256 ? launch_mixed_contig<8>(p, cfg.stream) : launch_mixed_contig<16>(p, cfg.stream);
-    } else {
-      // generic addressing (strided, or contiguous but unaligned or short)
-      const int T = pow2c((N + 7) / 8);
-      int W = 512 / T > 16 ? 16 : 512 / T;
-      if (T <= 32 && W * T > 256) W = 256 / T;
-      if (W * T < 32) W = 32 / T;
-      if (T <= 32)
-        e = launch_mixed_strided<8, 2>(p, T, W, cfg.stream);
-      else
-        e = launch_mixed_strided<8, 4>(p, T, W, cfg.stream);
-    }
+  } else if (e == cudaSuccess && direct) {
+    // direct FP64 solve of the promoted values
+    e = N <= 256 ? launch_contig_promoted<8>(p, cfg.stream) : launch_contig_promoted<16>(p, cfg.stream);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  } else if (e == cudaSuccess) {
+    e = launch_refinement<float>(p, cfg.stream);
   }
   if (e != cudaSuccess) return status_of(e);
-  if (cfg.blocking) {
+  if (!cfg.blocking) return TRID_STATUS_SUCCESS;
+  if (direct) {
     e = cudaStreamSynchronize(cfg.stream);
     if (e != cudaSuccess) return status_of(e);
-    MixedStats st{};
-    e = cudaMemcpyFromSymbol(&st, g_mixed_stats, sizeof(st));
-    if (e != cudaSuccess) return status_of(e);
-    if (iters_out) *iters_out = (int)st.iters;
-    if (correction_out) {
-      double v;
-      memcpy(&v, &st.corr_bits, sizeof(v));
-      *correction_out = v;
-    }
-    if (pivot_flag_take()) return TRID_STATUS_ZERO_PIVOT;
+    if (iters_out) *iters_out = 0;
+    if (correction_out) *correction_out = 0.0;
+    return pivot_flag_take() ? TRID_STATUS_ZERO_PIVOT : TRID_STATUS_SUCCESS;
   }
-  return TRID_STATUS_SUCCESS;
+  return finish_refinement(cfg, iters_out, correction_out);
+}
+
+EXTERN_C tridStatus_t tridDmtsvStridedBatchRefine(const TridParams *ctx, const double *a,
+                                                  const double *b, const double *c, double *d,
+                                                  int ndim, int solvedim, const int *dims_p,
+                                                  const int *pads_p, int max_iters, double tol,
+                                                  int *iters_out, double *correction_out) {
+  const TraceScope trace("tridDmtsvStridedBatchRefine");
+  (void)ctx;
+  if (iters_out) *iters_out = -1;
+  if (correction_out) *correction_out = -1.0;
+  MixedArgsT<double> p{};
+  bool empty = false;
+  tridStatus_t sts = make_mixed_args<double>(a, b, c, d, ndim, solvedim, dims_p, pads_p,
+                                             max_iters, tol, &p, &empty);
+  if (sts != TRID_STATUS_SUCCESS) return sts;
+  if (empty) {
+    if (iters_out) *iters_out = 0;
+    if (correction_out) *correction_out = 0.0;
+    return TRID_STATUS_SUCCESS;
+  }
+  sts = device_ready();
+  if (sts != TRID_STATUS_SUCCESS) return sts;
+  if (p.N > 512) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
+  const Settings &cfg = settings();
+  p.flag = pivot_flag_device();
+  if (cfg.blocking) pivot_flag_take();
+  MixedStats zero{};
+  cudaError_t e = cudaMemcpyToSymbolAsync(g_mixed_stats, &zero, sizeof(zero), 0,
+                                          cudaMemcpyHostToDevice, cfg.stream);
+  if (e == cudaSuccess) e = launch_refinement<double>(p, cfg.stream);
+  if (e != cudaSuccess) return status_of(e);
+  if (!cfg.blocking) return TRID_STATUS_SUCCESS;
+  return finish_refinement(cfg, iters_out, correction_out);
 }
