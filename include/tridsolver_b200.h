@@ -111,6 +111,18 @@ EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a
  * Longer systems always take tiles (512 rows double / 1024 rows float,
  * N <= 16384). */
 EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
+/* Failure-detection hook (process-wide; tests only). A warp holding one tile
+ * of a multi-tile system waits, bounded, for the warp that solves the
+ * system's second-level system to publish it. polls sets that bound (each
+ * poll sleeps about 128 ns; 0 restores the default of 2^22 polls, about half
+ * a second); withhold_publish != 0 makes the solving warp withhold its
+ * publication, so every such wait runs out. A wait that gives up leaves its
+ * tile unsolved, stops the launch's other waits at once, and makes a
+ * blocking ragged call return TRID_STATUS_EXECUTION_FAILED; the device
+ * context stays usable and later calls solve normally once the hook is
+ * reset. */
+EXTERN_C tridStatus_t tridRaggedSetWaitBound(unsigned long long polls, int withhold_publish);
+
 /* Copies the table in use (one entry per length class ceil(log2 N) = 0, 1,
  * ...: rows per lane of a warp per system, or 0 for tiles) and
  * returns the number of classes, or -1. */

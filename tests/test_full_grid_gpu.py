@@ -1,0 +1,81 @@
+"""GPU: the full BASELINE grids, elementwise, against the reference library.
+
+Every case of the drop-in sweep: 256^3 and 512^3 grids, FP64 and FP32,
+solvedim 0, 1 and 2, overwrite and Inc, with the benchmark's inputs
+(a, c ~ U(-0.5, 0.5), a = 0 on every system's first row and c = 0 on its
+last, b = 1 + |a| + |c| + U(0, 1), d ~ N(0, 1), u ~ N(0, 1)). Each result is
+compared in full with the reference's own CPU solver (scalar/src/cpu/
+trid_cpu.cpp, built from its sources into oracle/_ref; the plain-C
+restatement where that build is absent), elementwise at the reference
+tests' tolerances (FP64 abs = rel = 1e-11, FP32 abs 1e-6 / rel 1e-5,
+scalar/test/utils.hpp:14-17) and normwise at 1e-12 / 1e-5. The inputs of
+Inc's d are checked to be left untouched.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import tridsolver_b200 as tb
+from fixtures import allclose_ref
+from helpers import normwise
+from oracle.pyoracle import Reference, Restatement
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float64: 1e-12, np.float32: 1e-5}
+
+
+@pytest.fixture(scope="module")
+def checker():
+    try:
+        return Reference()
+    except FileNotFoundError:
+        return Restatement()
+
+
+def _inputs(n, solvedim, tdt, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    shape = (n, n, n)
+    tdim = 2 - solvedim
+    a = torch.rand(shape, generator=g, device="cuda", dtype=tdt) - 0.5
+    c = torch.rand(shape, generator=g, device="cuda", dtype=tdt) - 0.5
+    b = 1 + a.abs() + c.abs() + torch.rand(shape, generator=g, device="cuda", dtype=tdt)
+    a.narrow(tdim, 0, 1).zero_()
+    c.narrow(tdim, n - 1, 1).zero_()
+    d = torch.randn(shape, generator=g, device="cuda", dtype=tdt)
+    u = torch.randn(shape, generator=g, device="cuda", dtype=tdt)
+    return a, b, c, d, u
+
+
+@pytest.mark.parametrize("inc", [False, True], ids=["overwrite", "inc"])
+@pytest.mark.parametrize("solvedim", [0, 1, 2])
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("n", [256, 512])
+def test_full_grid_elementwise(n, dt, solvedim, inc, checker):
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    a, b, c, d, u = _inputs(n, solvedim, tdt, seed=1000 * n + 10 * solvedim + inc)
+    dims = [n] * 3
+    ha, hb, hc, hd, hu = (t.cpu().numpy().reshape(-1) for t in (a, b, c, d, u))
+    if inc:
+        fn = tb.tridDmtsvStridedBatchInc if dt == np.float64 else tb.tridSmtsvStridedBatchInc
+        st = fn(None, a, b, c, d, u, 3, solvedim, dims, dims)
+        out = u
+    else:
+        fn = tb.tridDmtsvStridedBatch if dt == np.float64 else tb.tridSmtsvStridedBatch
+        st = fn(None, a, b, c, d, 3, solvedim, dims, dims)
+        out = d
+    torch.cuda.synchronize()
+    assert st == 0
+    got = out.cpu().numpy().reshape(-1)
+    if inc:
+        assert torch.equal(d.cpu(), torch.from_numpy(hd.reshape(n, n, n))), "Inc wrote d"
+    del a, b, c, d, u, out
+    torch.cuda.empty_cache()
+    want_u = hu.copy() if inc else None
+    want_d = hd.copy()
+    checker.strided_batch(ha, hb, hc, want_d, dims, solvedim, u=want_u)
+    want = want_u if inc else want_d
+    assert normwise(got, want) <= TOL[dt]
+    ok, worst, diff = allclose_ref(want, got, dt)
+    assert ok, (worst, diff, want[worst], got[worst])

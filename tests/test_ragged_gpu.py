@@ -115,3 +115,61 @@ def test_release_scratch_between_calls(oracle):
     want = arrs[3].copy()
     oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
     assert np.max(np.abs(second - want)) / np.max(np.abs(want)) <= 1e-12
+
+
+def test_bounded_wait_runs_out_and_is_reported(oracle):
+    """Failure detection without a GPU fault: the warp that solves each
+    multi-tile system's second-level system withholds its publication (a
+    flag that nothing sets), so the other tiles' bounded waits run out. The
+    blocking call returns an error status, and the context stays usable: the
+    same batch then solves normally."""
+    lib = tb.load_library()
+    lengths = np.array([3000, 40, 9000, 700, 2048] * 8)  # multi-tile in both precisions
+    for dt in (np.float64, np.float32):
+        arrs, offs = _batch(lengths, dt, seed=8)
+        lib.tridRaggedSetWaitBound(1 << 14, 1)  # about 2 ms per wait
+        try:
+            st, _ = _run(arrs, offs, dt)
+        finally:
+            lib.tridRaggedSetWaitBound(0, 0)
+        assert st == tb.TridStatus.EXECUTION_FAILED
+        st, got = _run(arrs, offs, dt)
+        assert st == 0
+        want = arrs[3].copy()
+        oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
+        tol = 1e-12 if dt == np.float64 else 1e-5
+        assert np.max(np.abs(got.astype(np.float64) - want)) / np.max(np.abs(want)) <= tol
+
+
+@pytest.mark.parametrize("dt,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_bench_batch_of_200000_systems(dt, tol, oracle):
+    """The benchmark's ragged batch itself: 200,000 systems with lengths
+    floor(exp(U(ln 8, ln 16384))) (seed 0), about 4.3e8 elements, against
+    the oracle's per-system solve, over the batch and per system."""
+    rng = np.random.default_rng(0)
+    lengths = np.floor(np.exp(rng.uniform(np.log(8), np.log(16384), 200000))).astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
+    n = int(offs[-1])
+    g = torch.Generator(device="cuda").manual_seed(12)
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    ta = torch.rand(n, generator=g, device="cuda", dtype=tdt) - 0.5
+    tc = torch.rand(n, generator=g, device="cuda", dtype=tdt) - 0.5
+    tb_ = 1 + ta.abs() + tc.abs() + torch.rand(n, generator=g, device="cuda", dtype=tdt)
+    td = torch.randn(n, generator=g, device="cuda", dtype=tdt)
+    a, b, c, want = (t.cpu().numpy() for t in (ta, tb_, tc, td))
+    fn = tb.tridDmtsvRaggedBatch if dt == np.float64 else tb.tridSmtsvRaggedBatch
+    st = fn(None, ta, tb_, tc, td, torch.from_numpy(offs).cuda(), len(lengths))
+    torch.cuda.synchronize()
+    assert st == 0
+    del ta, tb_, tc
+    got = td.cpu().numpy()
+    del td
+    torch.cuda.empty_cache()
+    oracle.ragged(a, b, c, want, offs)
+    del a, b, c
+    diff = np.abs(got.astype(np.float64) - want)
+    assert diff.max() / np.abs(want).max() <= tol
+    # per system: the largest error relative to that system's own max |x|
+    smax = np.maximum.reduceat(np.abs(want), offs[:-1])
+    dmax = np.maximum.reduceat(diff, offs[:-1])
+    assert np.max(dmax / smax) <= 10 * tol

@@ -45,6 +45,7 @@ SYMBOLS = {
     "tridSmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
     "tridRaggedAutotune": (_I, [_I]),
     "tridRaggedTable": (_I, [_I, _IP, _I]),
+    "tridRaggedSetWaitBound": (_I, [ctypes.c_ulonglong, _I]),
     "tridDADIStep": (_I, [_P] * 7 + [ctypes.c_double, _I, _I, _I]),
     "tridSADIStep": (_I, [_P] * 7 + [ctypes.c_float, _I, _I, _I]),
     "tridDmtsvStridedBatchAdjoint": (_I, [_P] * 10 + [_I, _I, _IP, _IP]),

@@ -32,6 +32,7 @@
 // (scalar/src/cpu/trid_cpu.cpp:312-353) is the oracle for each system.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -72,6 +73,8 @@ template <typename R> struct RaggedArgs {
                                     // 3: the tile table was too small
   long long max_tiles;              // entries of tile_meta / tile_base / tile_rows / tile_fl
   bool vec16;                       // a, b, c, d all 16-byte aligned
+  unsigned wait_limit;              // polls before a wait gives up (kWaitLimit by default)
+  bool withhold;                    // failure-detection tests: never publish (waits run out)
 };
 
 // Release/acquire operations at device scope: a tile's second-level rows are
@@ -404,16 +407,17 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
       }
       __threadfence();
       __syncwarp();
-      if (lane == 0) atomicExch(&p.sys_ready[s], 1u);
+      if (lane == 0 && !p.withhold) atomicExch(&p.sys_ready[s], 1u);
     } else {
       unsigned ok = 1;
       if (lane == 0) {
-        // bounded: kWaitLimit polls, and none at all once any wait of this
-        // launch has given up (error != 0)
+        // bounded: p.wait_limit polls (kWaitLimit unless a test lowered
+        // it), and none at all once any wait of this launch has given up
+        // (error != 0)
         const volatile unsigned *err = p.error;
         unsigned it = 0;
         unsigned r = load_acquire(p.sys_ready + s);
-        while (r == 0u && *err == 0u && it < kWaitLimit) {
+        while (r == 0u && *err == 0u && it < p.wait_limit) {
           __nanosleep(128);
           ++it;
           r = load_acquire(p.sys_ready + s);
@@ -517,6 +521,11 @@ static void default_mtab(int *m) {
   }
 }
 
+// Failure-detection hooks (tridRaggedSetWaitBound): the wait bound in polls
+// (0: kWaitLimit) and whether second-level solutions are withheld.
+static std::atomic<unsigned long long> g_wait_polls{0};
+static std::atomic<int> g_withhold{0};
+
 template <typename R>
 static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t st) {
   for (int c = 0; c < kClasses; ++c) p.mtab[c] = mtab[c];
@@ -580,6 +589,11 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   p.max_tiles = max_tiles;
   p.counter = counter;
   p.error = error;
+  {
+    const unsigned long long lim = g_wait_polls.load(std::memory_order_relaxed);
+    p.wait_limit = lim == 0 ? kWaitLimit : (unsigned)(lim > 0xffffffffULL ? 0xffffffffULL : lim);
+    p.withhold = g_withhold.load(std::memory_order_relaxed) != 0;
+  }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -803,4 +817,10 @@ EXTERN_C int tridRaggedTable(int dtype_bytes, int *rows_per_lane, int nclasses) 
     n = cls + 1;
   }
   return n;
+}
+
+EXTERN_C tridStatus_t tridRaggedSetWaitBound(unsigned long long polls, int withhold_publish) {
+  g_wait_polls.store(polls, std::memory_order_relaxed);
+  g_withhold.store(withhold_publish != 0, std::memory_order_relaxed);
+  return TRID_STATUS_SUCCESS;
 }
