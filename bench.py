@@ -13,8 +13,10 @@ Inputs are seeded synthetic data with the distribution the configs name
 metric through the C ABI with host arrays (pinned host -> device copies of
 a, b, c, d and the device -> host copy of the result inside the timed
 region). `cpu_baseline` times the reference's own CPU library (oracle/_ref)
-on the host cores on a bounded slab of the same workload. With --impl
-reference only that CPU timing runs, as the reference arm.
+on the host cores on the same full grid, and `reference_gpu` the reference's
+own CUDA library (oracle/_ref, built for sm_100a) on the same B200: the two
+baseline legs, the only code here that runs anything under oracle/. With
+--impl reference only the CPU timing runs, as the reference arm.
 
 Multi-GPU: one process per GPU (torchrun); the solve shards by systems with
 no exchange, so every rank solves its own grid (weak scaling) and value is
@@ -55,9 +57,9 @@ def parse_args():
     ap.add_argument("--grid", default=None,
                     help="X,Y,Z grid instead of n^3 (smaller cases for profiling; x fastest)")
     ap.add_argument("--e2e-steps", type=int, default=8)
-    ap.add_argument("--cpu-planes", type=int, default=32,
-                    help="slab thickness of the CPU sample (planes of n*n)")
-    ap.add_argument("--cpu-steps", type=int, default=0, help="0 = as many as fit in ~10 s")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="0 = as many as fit in ~8 s")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference CUDA library's same-box timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
@@ -150,10 +152,11 @@ class ClockSampler:
 
 # ---- CPU reference timing ---------------------------------------------------------
 
-def cpu_reference_rate(n, planes, steps, dtype, time_budget=10.0):
-    """elements/s of the reference CPU library (oracle/_ref) on a slab sample:
-    x and y solves on n*n*planes, the z solve on n*planes*n (every system keeps
-    its full length n). Returns (rate, info dict)."""
+def cpu_reference_rate(n, steps, dtype, warmup=1, time_budget=8.0):
+    """elements/s of the reference CPU library (oracle/_ref) on the benchmark's
+    own workload: x, y and z solves of the full n^3 grid (d overwritten each
+    time), all host threads. steps <= 0: as many steps as fit in about
+    time_budget seconds. Returns (rate, info dict)."""
     import numpy as np
 
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
@@ -164,23 +167,24 @@ def cpu_reference_rate(n, planes, steps, dtype, time_budget=10.0):
 
     ref = Reference()
     npdt = np.float64 if dtype == "f64" else np.float32
-    m = n * n * planes
+    m = n * n * n
     rng = np.random.default_rng(1)
-    a = rng.uniform(-0.5, 0.5, m).astype(npdt)
-    c = rng.uniform(-0.5, 0.5, m).astype(npdt)
-    b = (1 + np.abs(a) + np.abs(c) + rng.uniform(0, 1, m)).astype(npdt)
+    a = (rng.random(m) - 0.5).astype(npdt)
+    c = (rng.random(m) - 0.5).astype(npdt)
+    b = (1 + np.abs(a) + np.abs(c) + rng.random(m)).astype(npdt)
     d = rng.standard_normal(m).astype(npdt)
-    plan = [([n, n, planes], 0), ([n, n, planes], 1), ([n, planes, n], 2)]
+    dims = [n, n, n]
 
     def step():
-        for dims, sd in plan:
+        for sd in range(3):
             ref.strided_batch(a, b, c, d, dims, sd)
 
-    step()  # warm-up (page faults, thread start)
-    t0 = time.perf_counter()
-    step()
-    one = time.perf_counter() - t0
+    for _ in range(max(1, warmup)):
+        step()  # page faults, thread start
     if steps <= 0:
+        t0 = time.perf_counter()
+        step()
+        one = time.perf_counter() - t0
         steps = max(2, min(2000, int(time_budget / max(one, 1e-6))))
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -188,11 +192,59 @@ def cpu_reference_rate(n, planes, steps, dtype, time_budget=10.0):
     el = time.perf_counter() - t0
     rate = 3 * m * steps / el
     info = {"cores": threads, "kind": "reference",
-            "sample": f"{steps} steps of x,y solves on {n}x{n}x{planes} and the z solve on "
-                      f"{n}x{planes}x{n} ({dtype}, reference scalar/src/cpu/trid_cpu.cpp "
-                      f"built -O3 -fopenmp, {ref.isa}), {el:.2f} s",
-            "lib": os.path.basename(ref.path)}
+            "sample": f"{steps} steps of x, y, z solves on the full {n}^3 grid ({dtype}, reference "
+                      f"scalar/src/cpu/trid_cpu.cpp built -O3 -fopenmp, {ref.isa}), {el:.2f} s",
+            "lib": os.path.basename(ref.path), "same_config": True}
     return rate, info
+
+
+def gpu_reference_rate(n, steps=10, warmup=3):
+    """The reference's own CUDA library (scalar/src/cuda/trid_cuda.cu, built
+    for sm_100a into oracle/_ref by oracle/Makefile) on the benchmark's
+    workload on the same B200: default opts (cuBLAS-transpose x path,
+    trid_strided_multidim y and z), blocking calls as its API makes them,
+    timed with CUDA events; a same-box comparator, never the measured
+    product. Per axis and per x, y, z step."""
+    import torch
+
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import ReferenceGPU
+
+    ref = ReferenceGPU()
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(1234)
+    shape = (n, n, n)
+    a = torch.rand(shape, generator=g, device=dev, dtype=torch.float64) - 0.5
+    c = torch.rand(shape, generator=g, device=dev, dtype=torch.float64) - 0.5
+    b = 1 + a.abs() + c.abs() + torch.rand(shape, generator=g, device=dev, dtype=torch.float64)
+    d = torch.randn(shape, generator=g, device=dev, dtype=torch.float64)
+    dims = [n, n, n]
+    stream = torch.cuda.current_stream()
+    per_axis = {}
+    for axis in range(3):
+        def call():
+            ref.strided_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), d.data_ptr(), dims, axis, 8)
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        per_axis["xyz"[axis]] = statistics.median(ts)
+    step_ms = sum(per_axis.values())
+    del a, b, c, d
+    torch.cuda.empty_cache()
+    return {"impl": "reference CUDA library scalar/src/cuda/trid_cuda.cu, default opts, sm_100a",
+            "lib": os.path.basename(ref.path), "grid": dims, "dtype": "f64",
+            "ms_per_axis": {k: round(v, 4) for k, v in per_axis.items()},
+            "ms_per_step": round(step_ms, 4), "value": 3 * n ** 3 / step_ms * 1e3,
+            "unit": UNIT, "steps": steps, "warmup": warmup}
 
 
 # ---- the GPU arm ------------------------------------------------------------------
@@ -723,14 +775,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        planes = args.cpu_planes
-        rate, info = cpu_reference_rate(args.n, planes, args.steps, args.dtype)
+        rate, info = cpu_reference_rate(args.n, args.steps, args.dtype, warmup=args.warmup)
         line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
                 "impl": "reference",
-                "config": {"workload": f"{args.n}^3 {args.dtype.upper()} solves along x, y, z, "
-                                       "sampled as slabs that keep every system's full length",
+                "config": {"workload": f"{args.n}^3 {args.dtype.upper()} solves along x, y, z "
+                                       "(d overwritten), the full grid each step",
                            "grid": [args.n] * 3},
                 "cpu_baseline": dict(info, value=rate, unit=UNIT),
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -752,8 +803,15 @@ def main():
 
         line["configs"] = run_configs(torch.device("cuda", local_rank), peaks()[0])
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, info = cpu_reference_rate(args.n, args.cpu_planes, args.cpu_steps, args.dtype)
+        rate, info = cpu_reference_rate(args.n, args.cpu_steps, args.dtype)
         line["cpu_baseline"] = dict(info, value=rate, unit=UNIT)
+    if rank == 0 and world == 1 and not args.no_ref_gpu and args.dtype == "f64" and args.n <= 512:
+        try:
+            line["reference_gpu"] = gpu_reference_rate(args.n)
+            line["reference_gpu"]["ours_over_reference_gpu"] = round(
+                line["value"] / line["reference_gpu"]["value"], 3)
+        except Exception as e:  # the comparator is optional
+            line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
     if world > 1:
         import torch
 

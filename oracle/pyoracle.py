@@ -1,12 +1,15 @@
 """ctypes bindings of the CPU checkers built by oracle/Makefile.
 
-ORACLE — test infrastructure only. Two checkers:
+ORACLE — test infrastructure only (checkers and the baseline legs of bench.py):
 
 * ``Restatement``: oracle/_build/liboracle.so, the plain-C restatement of the
   reference algorithm (trid_oracle.c, each function cites the reference).
 * ``Reference``: oracle/_ref/libtridcpu_ref_{avx512,avx2}.so, the reference's
   own scalar/src/cpu/trid_cpu.cpp compiled from its sources with the API
   symbols renamed ref_*. The AVX-512 build is used when this CPU has avx512f.
+* ``ReferenceGPU``: oracle/_ref/libtridcuda_ref.so, the reference's own CUDA
+  library built for sm_100a: a same-box comparator for the benchmark,
+  itself checked against the two above by tests/test_reference_gpu.py.
 
 All arrays are numpy, x-fastest (Fortran order for an ndim-shaped array).
 """
@@ -161,3 +164,54 @@ def normwise_error(x, ref):
     ref = np.asarray(ref, dtype=np.float64)
     den = np.max(np.abs(ref)) if ref.size else 1.0
     return float(np.max(np.abs(x - ref)) / (den if den > 0 else 1.0)) if ref.size else 0.0
+
+
+class _RefTridParams(ctypes.Structure):
+    """struct TridParams (scalar/include/trid_params.h:31-35)."""
+    _fields_ = [("mpi_params", ctypes.c_void_p), ("opts", ctypes.c_int * 3), ("sync", ctypes.c_int)]
+
+
+class ReferenceGPU:
+    """The reference's own CUDA library, scalar/src/cuda/trid_cuda.cu compiled
+    for sm_100a from its sources (oracle/_ref/libtridcuda_ref.so, API symbols
+    renamed ref_gpu_*). Takes device pointers; every call ends with the
+    library's own cudaDeviceSynchronize. Its x path keeps transpose scratch
+    sized in an int, so arrays must stay below 2^31 bytes; its vectorised
+    y/z path assumes a system count divisible by 4 (FP32) or 2 (FP64) and
+    dims[0] * sizeof a multiple of 16 whenever the pointers are aligned."""
+
+    def __init__(self, path=None):
+        path = path or os.path.join(REF_DIR, "libtridcuda_ref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle` where the reference tree exists")
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        for name in ("ref_gpu_tridDmtsvStridedBatch", "ref_gpu_tridSmtsvStridedBatch",
+                     "ref_gpu_tridDmtsvStridedBatchInc", "ref_gpu_tridSmtsvStridedBatchInc"):
+            fn = getattr(self.lib, name)
+            fn.restype = ctypes.c_int
+        self.ctx = _RefTridParams()  # opts 0: the library's defaults
+
+    def strided_batch(self, a, b, c, d, dims, solvedim, dtype_bytes, pads=None, u=None, opts=None):
+        """a, b, c, d, u: device addresses (ints). d <- x, or u += x."""
+        pads = dims if pads is None else pads
+        n = 1
+        for v in pads:
+            n *= int(v)
+        if n * dtype_bytes >= 2 ** 31:
+            raise ValueError("arrays of 2^31 bytes or more overflow the reference's scratch size")
+        if opts is not None:
+            for i, v in enumerate(opts):
+                self.ctx.opts[i] = int(v)
+        p = "D" if dtype_bytes == 8 else "S"
+        vp = ctypes.c_void_p
+        if u is None:
+            rc = getattr(self.lib, f"ref_gpu_trid{p}mtsvStridedBatch")(
+                ctypes.byref(self.ctx), vp(a), vp(b), vp(c), vp(d), len(dims), int(solvedim),
+                _ints(dims), _ints(pads))
+        else:
+            rc = getattr(self.lib, f"ref_gpu_trid{p}mtsvStridedBatchInc")(
+                ctypes.byref(self.ctx), vp(a), vp(b), vp(c), vp(d), vp(u), len(dims),
+                int(solvedim), _ints(dims), _ints(pads))
+        if rc != 0:
+            raise ValueError(f"reference GPU rc={rc}")

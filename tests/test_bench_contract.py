@@ -15,7 +15,7 @@ def _run(env_extra=None):
     env = dict(os.environ)
     env.update(env_extra or {})
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                           "--n", "64", "--cpu-planes", "8", "--steps", "2", "--warmup", "1"],
+                           "--n", "64", "--steps", "2", "--warmup", "1"],
                           capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
 
 
@@ -32,10 +32,10 @@ def test_reference_arm_line():
         assert key in line, key
     assert line["impl"] == "reference"
     assert line["value"] > 0 and line["steps"] == 2 and line["warmup"] == 1
-    assert "workload" in line["config"]
+    assert "workload" in line["config"] and line["config"]["grid"] == [64, 64, 64]
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"]
-    assert cb["unit"] == line["unit"] and cb["sample"]
+    assert cb["unit"] == line["unit"] and cb["sample"] and cb["same_config"]
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
