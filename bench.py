@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument("--n", type=int, default=512, help="grid edge (512 = the benchmark)")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--only-config", default=None,
-                    choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint", "dist"],
+                    choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint", "dist",
+                             "long", "autotune"],
                     help="run just one of the other configurations and print its JSON (profiling)")
     ap.add_argument("--ragged-systems", type=int, default=200000,
                     help="systems in the ragged configuration (200000 = the benchmark)")
@@ -648,6 +649,67 @@ def config_dist(dev, hbm, n=512):
             "results": out}
 
 
+def config_long(dev, hbm):
+    """Few, long FP64 systems (the long path: chunk reduction to scratch,
+    recursive solve of the reduced batch, substitution), along x (contiguous)
+    and z (rows a plane apart). Its byte floor is 9 words per element: a, b,
+    c, d read in the reduction and again in the substitution, x written."""
+    import torch
+    import tridsolver_b200 as tb
+    stream = torch.cuda.current_stream()
+    out = []
+    for dims, axis, label in (([1 << 20, 64], 0, "64 x 2^20 rows, x"),
+                              ([65536, 1024], 0, "1024 x 65536 rows, x"),
+                              ([8, 8, 1 << 20], 2, "64 x 2^20 rows, z"),
+                              ([32, 32, 65536], 2, "1024 x 65536 rows, z")):
+        shape = tuple(reversed(dims))
+        a, b, c, d = _system(shape, torch.float64, dev, 31)
+        nd = len(dims)
+        x = d.clone()
+        ms = _timed(lambda: tb.tridDmtsvStridedBatch(None, a, b, c, x, nd, axis, dims, dims), 5,
+                    stream)
+        n = a.numel()
+        gbs9 = 9 * 8 * n / ms / 1e6
+        out.append({"case": label, "dims": dims, "solvedim": axis, "ms": round(ms, 4),
+                    "elements_per_s": n / ms * 1e3, "plan": tb.describe_plan(8, dims, axis),
+                    "bytes_per_element": 72, "hbm_gbs_at_9_words": round(gbs9, 1),
+                    "frac_of_9_word_floor": round(gbs9 / hbm, 4)})
+        del a, b, c, d, x
+        torch.cuda.empty_cache()
+    return out
+
+
+def config_autotune(dev, hbm):
+    """tridAutotune on the drop-in grids: for each shape the built-in plan and
+    the tuned plan (the fastest of every applicable plan on this device),
+    both timed as the solve then runs."""
+    import torch
+    import tridsolver_b200 as tb
+    stream = torch.cuda.current_stream()
+    out = []
+    for n, dt, es in ((512, torch.float64, 8), (256, torch.float32, 4), (256, torch.float64, 8)):
+        shape = (n, n, n)
+        a, b, c, d = _system(shape, dt, dev, 41)
+        dims = [n] * 3
+        solve = tb.tridDmtsvStridedBatch if es == 8 else tb.tridSmtsvStridedBatch
+        for axis in range(3):
+            tb.autotune_reset()
+            plan0 = tb.describe_plan(es, dims, axis)
+            t0 = _timed(lambda: solve(None, a, b, c, d, 3, axis, dims, dims), 10, stream)
+            tb.set_blocking(True)
+            _, plan1 = tb.autotune(es, dims, axis)
+            tb.set_blocking(False)
+            t1 = _timed(lambda: solve(None, a, b, c, d, 3, axis, dims, dims), 10, stream)
+            gbs = 5 * es * n ** 3 / t1 / 1e6
+            out.append({"grid": dims, "dtype": "f64" if es == 8 else "f32", "axis": "xyz"[axis],
+                        "builtin_plan": plan0, "builtin_ms": round(t0, 4), "tuned_plan": plan1,
+                        "tuned_ms": round(t1, 4), "tuned_frac": round(gbs / hbm, 4)})
+        tb.autotune_reset()
+        del a, b, c, d
+        torch.cuda.empty_cache()
+    return out
+
+
 def config_adjoint(dev, n=256, probes=1000):
     """Adjoint along y on 256^3 FP64: time against the forward solve; gradient
     entries against central finite differences (h = 1e-6) of L = sum(w x)."""
@@ -738,6 +800,8 @@ def run_configs(dev, hbm):
                      ("adi_512x512x128_f32_1000", lambda: config_adi(dev, hbm, (128, 512, 512), 1000,
                                                                       "f32")),
                      ("adjoint", lambda: config_adjoint(dev)),
+                     ("long_systems", lambda: config_long(dev, hbm)),
+                     ("autotune", lambda: config_autotune(dev, hbm)),
                      ("dist_512_f64", lambda: config_dist(dev, hbm)),
                      ("adi_backprop", lambda: config_adi_backprop(dev))):
         try:
@@ -765,7 +829,9 @@ def main():
               "precision": lambda: config_precision(dev, args.n, grid),
               "ragged": lambda: config_ragged(dev, hbm, args.ragged_systems),
               "adjoint": lambda: config_adjoint(dev),
-              "dist": lambda: config_dist(dev, hbm)}[args.only_config]
+              "dist": lambda: config_dist(dev, hbm),
+              "long": lambda: config_long(dev, hbm),
+              "autotune": lambda: config_autotune(dev, hbm)}[args.only_config]
         print(json.dumps({"config": args.only_config, "result": fn()}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -68,6 +68,26 @@ EXTERN_C tridStatus_t tridSetTracing(int on);
 #define TRID_FAMILY_LONG 2
 EXTERN_C tridStatus_t tridForcePlan(int family, int rows_per_thread);
 
+/* Autotuner. Counterpart of the reference's fixed Thomas-PCR length tables
+ * (scalar/src/cuda/trid_thomaspcr.hpp:537-598), measured instead of fixed:
+ * times every plan that applies to the given shape (pure PCR; the hybrid at
+ * rows per thread 2..32, from thread-per-system Thomas to a warp per system;
+ * for strided batches the register-tile kernel, the 128- and 256-byte
+ * streaming kernels and TMA tiles; the long multi-block path) on synthetic
+ * data of that shape allocated for the call (cudaMalloc; blocking, typically
+ * well under a second), and keeps the fastest for the shape's class on the
+ * current device: precision, Inc or not (inc != 0), layout (contiguous;
+ * strided with rows under 64 KiB apart; strided with rows further apart),
+ * whether at least 32 systems run along the fastest dimension, and the
+ * length bucket ceil(log2 N). Later automatic plan choices for that class
+ * use it (tridForce* settings still take precedence). *best_ms and plan
+ * (a tridDescribePlan string, plan_len bytes) receive the winner when not
+ * NULL. tridAutotuneReset forgets the current device's choices. */
+EXTERN_C tridStatus_t tridAutotune(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                                   const int *pads, int inc, float *best_ms, char *plan,
+                                   int plan_len);
+EXTERN_C tridStatus_t tridAutotuneReset(void);
+
 /* Pins the number of neighbouring systems one thread block of the strided
  * hybrid handles (a power of two; 0 restores the automatic choice). */
 EXTERN_C tridStatus_t tridForceSystemsPerBlock(int systems);

@@ -177,7 +177,8 @@ def test_release_scratch_reports_missing_device():
     (8, [64, 64], 1, "hybrid M=8 T=8 W=32"),
     (8, [8, 8, 1024], 2, "hybrid M=8 T=128 W=4"),
     (4, [1024, 8], 0, "hybrid M=32 T=32"),
-    (4, [256, 256, 256], 0, "hybrid M=8 T=32 W=1 smem"),
+    (4, [256, 256, 256], 0, "hybrid M=16 T=16 W=1 vec"),
+    (4, [128, 256, 2], 0, "hybrid M=8 T=16 W=1 vec"),
     (8, [256, 256, 256], 0, "hybrid M=8 T=32 W=1 smem"),
     (8, [100000], 0, "long"),
     (8, [5, 7], 1, "hybrid M=8 T=1"),

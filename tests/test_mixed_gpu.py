@@ -56,7 +56,10 @@ def _problem(dims, solvedim, margin, seed):
 
 
 SHAPES = [([512, 4, 3], 0), ([256, 8, 2], 0), ([200, 7], 0), ([33, 3], 0), ([1], 0),
-          ([16, 512, 2], 1), ([10, 300], 1), ([24, 3, 512], 2), ([40, 5, 256], 2), ([9, 2, 7], 2)]
+          ([16, 512, 2], 1), ([10, 300], 1), ([24, 3, 512], 2), ([40, 5, 256], 2), ([9, 2, 7], 2),
+          # rows a plane (>= 64 KiB) apart: the wide kernel's promoted form,
+          # full and partial 32-system groups
+          ([32, 256, 300], 2), ([20, 512, 130], 2), ([48, 256, 512], 2)]
 
 
 def _problem64(dims, solvedim, margin, seed):

@@ -46,6 +46,9 @@ SYMBOLS = {
     "tridRaggedAutotune": (_I, [_I]),
     "tridRaggedTable": (_I, [_I, _IP, _I]),
     "tridRaggedSetWaitBound": (_I, [ctypes.c_ulonglong, _I]),
+    "tridAutotune": (_I, [_I, _I, _I, _IP, _IP, _I, ctypes.POINTER(ctypes.c_float), ctypes.c_char_p,
+                          _I]),
+    "tridAutotuneReset": (_I, []),
     "tridDADIStep": (_I, [_P] * 7 + [ctypes.c_double, _I, _I, _I]),
     "tridSADIStep": (_I, [_P] * 7 + [ctypes.c_float, _I, _I, _I]),
     "tridDmtsvStridedBatchAdjoint": (_I, [_P] * 10 + [_I, _I, _IP, _IP]),

@@ -176,6 +176,26 @@ def ragged_autotune(dtype_bytes):
         raise TridError(st, "tridRaggedAutotune")
 
 
+def autotune(dtype_bytes, dims, solvedim, pads=None, inc=False):
+    """tridAutotune: time every applicable plan for this shape on the current
+    device and keep the fastest for its shape class. Returns (ms, plan)."""
+    pads = dims if pads is None else pads
+    ms = ctypes.c_float(-1.0)
+    buf = ctypes.create_string_buffer(96)
+    st = _lib.load().tridAutotune(int(dtype_bytes), len(dims), int(solvedim), _ints(dims),
+                                  _ints(pads), int(bool(inc)), ctypes.byref(ms), buf, 96)
+    if st != 0:
+        raise TridError(st, "tridAutotune")
+    return ms.value, buf.value.decode()
+
+
+def autotune_reset():
+    """tridAutotuneReset: forget the current device's tuned choices."""
+    st = _lib.load().tridAutotuneReset()
+    if st != 0:
+        raise TridError(st, "tridAutotuneReset")
+
+
 def ragged_table(dtype_bytes):
     """Rows per lane by length class (index = ceil(log2 N)) for warp items."""
     buf = (ctypes.c_int * 32)()

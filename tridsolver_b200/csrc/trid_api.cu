@@ -95,7 +95,7 @@ TraceScope::~TraceScope() {
 }
 
 // ---- device check ----------------------------------------------------------
-static tridStatus_t check_device() {
+tridStatus_t check_device() {
   static thread_local int checked_dev = -1;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -126,9 +126,9 @@ tridStatus_t status_of(cudaError_t e) {
 // Validates the strided-batch arguments and fills a BatchArgs. Returns
 // SUCCESS with *empty = true when there is nothing to solve.
 template <typename R>
-static tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, bool inc, int ndim,
-                               int solvedim, const int *dims_p, const int *pads_p,
-                               BatchArgs<R> *out, bool *empty) {
+tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, bool inc, int ndim,
+                        int solvedim, const int *dims_p, const int *pads_p, BatchArgs<R> *out,
+                        bool *empty) {
   if (ndim < 1 || ndim > MAXDIM || solvedim < 0 || solvedim >= ndim || !dims_p || !pads_p)
     return TRID_STATUS_INVALID_VALUE;
   long long dims[3] = {1, 1, 1}, pads[3] = {1, 1, 1};
@@ -175,6 +175,12 @@ static tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, b
   *out = p;
   return TRID_STATUS_SUCCESS;
 }
+template tridStatus_t make_batch<double>(const double *, const double *, const double *, double *,
+                                         double *, bool, int, int, const int *, const int *,
+                                         BatchArgs<double> *, bool *);
+template tridStatus_t make_batch<float>(const float *, const float *, const float *, float *, float *,
+                                        bool, int, int, const int *, const int *, BatchArgs<float> *,
+                                        bool *);
 
 template <typename R, bool INC>
 static tridStatus_t solve_strided(const TridParams *ctx, const R *a, const R *b, const R *c, R *d,

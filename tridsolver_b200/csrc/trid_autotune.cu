@@ -1,0 +1,245 @@
+// Autotuner of strided and contiguous batches: per shape class, the fastest
+// of every plan that applies, measured on this device.
+//
+// The reference chooses its Thomas-PCR kernels by fixed length tables
+// (scalar/src/cuda/trid_thomaspcr.hpp:537-598: register-chunk size by
+// length bucket, one table per layout). Here the choice is measured: for a
+// shape given by the caller, tridAutotune times each candidate plan on
+// synthetic data of that shape and keeps the fastest for the shape's class:
+//   precision, Inc or not, layout (contiguous; strided with rows less than
+//   64 KiB apart, as y solves; strided with rows further apart, as z
+//   solves), whether at least 32 systems run along the fastest dimension,
+//   and the length bucket ceil(log2 N).
+// Candidates span the families: pure PCR (one row per thread, N <= 32);
+// the partition hybrid at every rows-per-thread M in {2, 4, 8, 16, 32}
+// (T = 1 is thread-per-system Thomas, T = 32 a warp per system; strided
+// batches up to 128 chunks, a block per system); for strided batches the
+// register-tile kernel, the 128-byte and the wide (256-byte) streaming
+// kernels and TMA tiles; and the long multi-block path. Ties keep the
+// built-in choice. Later automatic plan choices for the same class on this
+// device use the recorded recipe; tridForce* settings still take
+// precedence, and tridAutotuneReset forgets the recipes.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "trid_internal.h"
+#include "tridsolver_b200.h"
+
+namespace trid {
+
+namespace {
+
+constexpr int kMaxDev = 64;
+
+// shape class: element size, Inc, layout (0 contiguous, 1 rows < 64 KiB
+// apart, 2 rows further apart), n0 >= 32, ceil(log2 N)
+using Key = std::tuple<int, int, int, int, int>;
+
+std::mutex g_mu;
+std::map<Key, Forces> g_tuned[kMaxDev];
+
+template <typename R> Key key_of(const BatchArgs<R> &p) {
+  const int layout = p.stride == 1 ? 0 : (p.stride * (long long)sizeof(R) < (1LL << 16) ? 1 : 2);
+  int lg = 0;
+  while ((1LL << lg) < p.N) ++lg;
+  return Key((int)sizeof(R), p.u ? 1 : 0, layout, layout != 0 && p.n0 >= 32 ? 1 : 0, lg);
+}
+
+int current_device() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return dev >= 0 && dev < kMaxDev ? dev : -1;
+}
+
+template <typename R> __global__ void fill_kernel(R *a, R *b, R *c, R *d, R *u, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    // diagonally dominant rows, values that neither grow nor vanish under
+    // repeated solves
+    const R t = R((i * 2654435761LL) & 1023) * R(1.0 / 1024);
+    a[i] = R(-0.25) * t;
+    c[i] = R(-0.25) * (R(1) - t);
+    b[i] = R(1);
+    d[i] = t - R(0.5);
+    if (u) u[i] = R(0);
+  }
+}
+
+// The candidate recipes for a batch (duplicates removed by plan).
+template <typename R> std::vector<Forces> candidates(const BatchArgs<R> &p) {
+  std::vector<Forces> out;
+  out.push_back(Forces{});  // the built-in choice
+  if (p.N <= 32) {
+    Forces f;
+    f.family = TRID_FAMILY_PCR;
+    out.push_back(f);
+  }
+  for (int m : {2, 4, 8, 16, 32}) {
+    Forces f;
+    f.family = TRID_FAMILY_HYBRID;
+    f.m = m;
+    if (p.stride != 1) f.stream = 0;  // the register-tile kernel
+    out.push_back(f);
+  }
+  if (p.stride != 1) {
+    for (int mode : {1, 2}) {
+      Forces f;
+      f.stream = mode;
+      out.push_back(f);
+    }
+    for (int m : {8, 16}) {
+      Forces f;
+      f.m = m;
+      f.tma = 1;
+      f.stream = 0;
+      out.push_back(f);
+    }
+  }
+  if (p.N > 64) {
+    for (int m : {8, 16}) {
+      Forces f;
+      f.family = TRID_FAMILY_LONG;
+      f.m = m;
+      out.push_back(f);
+    }
+  }
+  return out;
+}
+
+template <typename R, bool INC>
+tridStatus_t autotune_shape(int ndim, int solvedim, const int *dims, const int *pads, float *best_ms,
+                            char *best_desc, int desc_len) {
+  tridStatus_t st = check_device();
+  if (st != TRID_STATUS_SUCCESS) return st;
+  const int dev = current_device();
+  if (dev < 0) return TRID_STATUS_INTERNAL_ERROR;
+  // the padded extent of the shape
+  if (ndim < 1 || ndim > MAXDIM || !dims || !pads) return TRID_STATUS_INVALID_VALUE;
+  long long extent = 1;
+  for (int i = 0; i < ndim; ++i) extent *= (i < ndim - 1 ? pads[i] : dims[i]);
+  if (extent <= 0) return TRID_STATUS_INVALID_VALUE;
+  const size_t bytes = (size_t)extent * sizeof(R);
+  R *buf = nullptr;
+  cudaStream_t s = settings().stream;
+  cudaError_t e = cudaMalloc((void **)&buf, bytes * (INC ? 5 : 4));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return TRID_STATUS_ALLOC_FAILED;
+  }
+  R *a = buf, *b = buf + extent, *c = b + extent, *d = c + extent, *u = INC ? d + extent : nullptr;
+  fill_kernel<R><<<1024, 256, 0, s>>>(a, b, c, d, u, extent);
+  BatchArgs<R> p;
+  bool empty = false;
+  st = make_batch<R>(a, b, c, d, u, INC, ndim, solvedim, dims, pads, &p, &empty);
+  if (st != TRID_STATUS_SUCCESS || empty) {
+    cudaFree(buf);
+    return st;
+  }
+  p.flag = nullptr;
+  const bool al = vec_aligned<R>(p);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  Forces best_f;
+  std::string best_d;
+  std::vector<std::string> seen;
+  for (const Forces &f : candidates<R>(p)) {
+    const Plan plan = choose_plan_forced<R>(p, al, f);
+    const std::string desc = plan.describe();
+    bool dup = false;
+    for (const std::string &x : seen) dup |= x == desc;
+    if (dup) continue;
+    seen.push_back(desc);
+    // two warm-up launches, then the mean of repeated launches over about
+    // 20 ms (at least 3)
+    cudaError_t le = launch_batch<R, INC>(p, plan, s);
+    if (le == cudaSuccess) le = launch_batch<R, INC>(p, plan, s);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+    if (le != cudaSuccess) {
+      cudaGetLastError();  // a candidate that does not apply (launch refused)
+      continue;
+    }
+    float ms = 0.f;
+    int reps = 3;
+    for (int round = 0; round < 2; ++round) {
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps; ++r) launch_batch<R, INC>(p, plan, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      if (round == 0) reps = ms > 0.f ? (int)fminf(200.f, fmaxf(3.f, 20.f / ms)) : 3;
+    }
+    // ties (within 1%) keep the earlier candidate, the built-in choice first
+    if (ms > 0.f && ms < 0.99f * best) {
+      best = ms;
+      best_f = f;
+      best_d = desc;
+    }
+  }
+  e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (e != cudaSuccess) return status_of(e);
+  if (best >= 1e30f) return TRID_STATUS_EXECUTION_FAILED;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_tuned[dev][key_of(p)] = best_f;
+  }
+  if (best_ms) *best_ms = best;
+  if (best_desc && desc_len > 0) {
+    strncpy(best_desc, best_d.c_str(), (size_t)desc_len - 1);
+    best_desc[desc_len - 1] = '\0';
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+template <typename R> void tuned_forces(const BatchArgs<R> &p, Forces *f) {
+  const int dev = current_device();
+  if (dev < 0) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_tuned[dev].empty()) return;
+  auto it = g_tuned[dev].find(key_of(p));
+  if (it != g_tuned[dev].end()) *f = it->second;
+}
+
+template void tuned_forces<double>(const BatchArgs<double> &, Forces *);
+template void tuned_forces<float>(const BatchArgs<float> &, Forces *);
+
+}  // namespace trid
+
+using namespace trid;
+
+EXTERN_C tridStatus_t tridAutotune(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                                   const int *pads, int inc, float *best_ms, char *plan,
+                                   int plan_len) {
+  const TraceScope trace("tridAutotune");
+  if (dtype_bytes == 8)
+    return inc ? autotune_shape<double, true>(ndim, solvedim, dims, pads, best_ms, plan, plan_len)
+               : autotune_shape<double, false>(ndim, solvedim, dims, pads, best_ms, plan, plan_len);
+  if (dtype_bytes == 4)
+    return inc ? autotune_shape<float, true>(ndim, solvedim, dims, pads, best_ms, plan, plan_len)
+               : autotune_shape<float, false>(ndim, solvedim, dims, pads, best_ms, plan, plan_len);
+  return TRID_STATUS_INVALID_VALUE;
+}
+
+EXTERN_C tridStatus_t tridAutotuneReset(void) {
+  const int dev = current_device();
+  if (dev < 0) return TRID_STATUS_NOT_INITIALIZED;
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_tuned[dev].clear();
+  return TRID_STATUS_SUCCESS;
+}

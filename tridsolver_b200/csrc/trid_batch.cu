@@ -51,6 +51,10 @@ static bool hybrid_supported(bool contig, int M, int T) {
 template <typename R>
 static int default_m(int N, bool contig) {
   if (contig) {
+    // FP32 systems of 129-256 rows: 16 lanes of 16 rows with 16-byte loads
+    // (two systems per warp) measured faster than a warp per system staged
+    // through shared memory (256^3 x: 0.055 vs 0.071 ms, tridAutotune)
+    if (sizeof(R) == 4 && N > 128 && N <= 256) return 16;
     if (N <= 256) return 8;
     if (N <= 512) return 16;
     return 32;
@@ -61,12 +65,27 @@ static int default_m(int N, bool contig) {
 
 template <typename R>
 Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
-  const Settings &st = settings();
+  Forces f;
+  if (honour_force) {
+    const Settings &st = settings();
+    f.family = st.force_family;
+    f.m = st.force_m;
+    f.w = st.force_w;
+    f.tma = st.force_tma;
+    f.stream = st.force_stream;
+  }
+  // nothing forced: the autotuner's choice for this shape class, if any
+  if (!f.any()) tuned_forces<R>(p, &f);
+  return choose_plan_forced<R>(p, aligned16, f);
+}
+
+template <typename R>
+Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f) {
   Plan plan;
   const int N = p.N;
   const bool contig = p.stride == 1;
-  int fam = honour_force ? st.force_family : TRID_FAMILY_AUTO;
-  int M = honour_force ? st.force_m : 0;
+  int fam = f.family;
+  int M = f.m;
   if (fam == TRID_FAMILY_PCR && N > 32) fam = TRID_FAMILY_HYBRID, M = 0;
   if (fam == TRID_FAMILY_PCR) {
     plan.family = fam;
@@ -96,7 +115,7 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         const int wmin = 32 / T > 1 ? 32 / T : 1;
         const int n0p = pow2_ceil(p.n0);
         if (W > n0p) W = n0p;
-        if (honour_force && st.force_w > 0) W = st.force_w;
+        if (f.w > 0) W = f.w;
         if (W < wmin) W = wmin;
         const int tmax = (T > 32 || M * (int)sizeof(R) <= 64) ? 512 : 256;
         if (W * T > tmax) W = tmax / T;
@@ -104,9 +123,9 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         // persistent streaming kernel for 64 < N <= 512: 128-byte row
         // segments, 512 threads (32 chunks of FP64 rows, 16 of FP32 rows)
         // and loads kept in flight across groups
-        const int fs = honour_force ? st.force_stream : -1;
-        const bool want_tma = honour_force && st.force_tma == 1;
-        const int fm = honour_force ? st.force_m : 0;
+        const int fs = f.stream;
+        const bool want_tma = f.tma == 1;
+        const int fm = f.m;
         // the wide form (256-byte groups, state in tensor memory) for FP64
         // rows a whole plane apart (>= 64 KiB: z solves), where the rate of
         // row segments limits 128-byte groups (512^3 z: 0.88 vs 1.11 ms, Inc
@@ -151,11 +170,11 @@ Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force) {
         // TMA tiles (two stages when they fit), at most 256 threads per CTA.
         // Opt-in: with rows of 32-64 bytes the tile loads are limited by the
         // rate of box rows, and measure slower than per-thread loads.
-        const int ft = honour_force ? st.force_tma : -1;
+        const int ft = f.tma;
         if (ft == 1 && (M == 8 || (M == 16 && sizeof(R) == 4)) && T <= 128) {
           const int wmin_tma = 16 / (int)sizeof(R);
-          int wt = (honour_force && st.force_w > 0) ? st.force_w : 2 * wmin_tma;
-          if (!(honour_force && st.force_w > 0)) {
+          int wt = f.w > 0 ? f.w : 2 * wmin_tma;
+          if (!(f.w > 0)) {
             // widest group (up to 16) that keeps two stages and covers n0
             for (int cand = wt * 2; cand <= 16; cand *= 2) {
               int rb, nb, stg;
@@ -343,6 +362,7 @@ cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t s
 
 #define INSTANTIATE(R)                                                                  \
   template Plan choose_plan<R>(const BatchArgs<R> &, bool, bool);                           \
+  template Plan choose_plan_forced<R>(const BatchArgs<R> &, bool, const Forces &);          \
   template bool vec_aligned<R>(const BatchArgs<R> &);                                 \
   template cudaError_t launch_batch<R, false>(const BatchArgs<R> &, const Plan &,     \
                                               cudaStream_t);                          \

@@ -64,13 +64,41 @@ class TraceScope {
 unsigned *pivot_flag_device();
 bool pivot_flag_take();  // reads and clears the word of the current device
 
-// honour_force: apply the calling thread's tridForcePlan setting (top-level
-// calls only; internal recursions use the automatic table).
 // CUDA error -> library status (trid_api.cu).
 tridStatus_t status_of(cudaError_t e);
+// The current device is an sm_100 GPU (trid_api.cu).
+tridStatus_t check_device();
+// Validates the strided-batch arguments and fills a BatchArgs; SUCCESS with
+// *empty = true when there is nothing to solve (trid_api.cu).
+template <typename R>
+tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, bool inc, int ndim,
+                        int solvedim, const int *dims_p, const int *pads_p, BatchArgs<R> *out,
+                        bool *empty);
 
+// Plan choices that override the built-in table: the calling thread's
+// tridForce* settings, or an autotuned recipe (family, rows per thread,
+// streaming form, TMA; all automatic by default).
+struct Forces {
+  int family = TRID_FAMILY_AUTO;
+  int m = 0;
+  int w = 0;
+  int tma = -1;
+  int stream = -1;
+  bool any() const { return family != TRID_FAMILY_AUTO || m != 0 || w != 0 || tma != -1 || stream != -1; }
+};
+
+// honour_force: apply the calling thread's tridForce* settings (top-level
+// calls only; internal recursions do not). With nothing forced, the
+// autotuner's recipe for the batch's shape class is used when one exists
+// (tridAutotune), else the built-in table.
 template <typename R>
 Plan choose_plan(const BatchArgs<R> &p, bool aligned16, bool honour_force = true);
+template <typename R>
+Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f);
+// The autotuned recipe for p's shape class on the current device (trid_autotune.cu);
+// leaves *f untouched when there is none.
+template <typename R>
+void tuned_forces(const BatchArgs<R> &p, Forces *f);
 
 // Enqueues the solve of batch p on `st` (no synchronisation).
 template <typename R, bool INC>
@@ -102,6 +130,9 @@ template <typename R> int wide_rows_per_thread(int N);
 template <typename R> int wide_width();
 template <typename R, bool INC>
 cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st);
+// The wide kernel in FP64 arithmetic on FP32-stored a, b, c.
+cudaError_t launch_strided_wide_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
+                                         cudaStream_t st);
 // The streaming kernel in FP64 arithmetic on FP32-stored a, b, c.
 template <int M>
 cudaError_t launch_strided_stream_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,

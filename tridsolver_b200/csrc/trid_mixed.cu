@@ -929,9 +929,16 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchMixed(const TridParams *ctx, const fl
     q.stride = p.stride;
     q.flag = p.flag;
     const CoefPtrs<float> cf{a, b, c};
-    e = N <= 128   ? launch_strided_stream_promoted<4>(q, cf, cfg.stream)
-        : N <= 256 ? launch_strided_stream_promoted<8>(q, cf, cfg.stream)
-                   : launch_strided_stream_promoted<16>(q, cf, cfg.stream);
+    // rows a plane apart (z solves) with at least half a 32-system group:
+    // the wide kernel (FP32 coefficient rows of 128 bytes, d of 256), else
+    // the 128-byte streaming kernel
+    const bool zlike = p.stride * (long long)sizeof(double) >= (1LL << 16);
+    if (zlike && 2 * p.n0 >= wide_width<double>())
+      e = launch_strided_wide_promoted(q, cf, cfg.stream);
+    else
+      e = N <= 128   ? launch_strided_stream_promoted<4>(q, cf, cfg.stream)
+          : N <= 256 ? launch_strided_stream_promoted<8>(q, cf, cfg.stream)
+                     : launch_strided_stream_promoted<16>(q, cf, cfg.stream);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   } else if (e == cudaSuccess && direct) {
     // direct FP64 solve of the promoted values

@@ -32,6 +32,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "trid_internal.h"
 
 namespace trid {
@@ -135,13 +137,22 @@ __device__ __forceinline__ void tmem_row(const uint32_t (&v)[NW], int i, R &af, 
 
 // Row `row` at element offset o: identity rows outside the system, a[0] and
 // c[N-1] forced to zero. Loads are cached in L2 only: nothing is read twice.
-template <typename R, bool INC>
-__device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, long long o, bool valid, int row, R &a,
-                                              R &b, R &c, R &d) {
+// CR: the coefficients' storage type; with CR = float and R = double (the
+// promoted solve of tridDmtsvStridedBatchMixed) a, b, c are read from cf as
+// FP32 and the solve runs in FP64 on their exact promoted values.
+template <typename R, typename CR>
+__device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, const CoefPtrs<CR> &cf, long long o,
+                                              bool valid, int row, R &a, R &b, R &c, R &d) {
   if (valid) {
-    a = row == 0 ? R(0) : __ldcg(p.a + o);
-    c = row == p.N - 1 ? R(0) : __ldcg(p.c + o);
-    b = __ldcg(p.b + o);
+    if constexpr (std::is_same<CR, R>::value) {
+      a = row == 0 ? R(0) : __ldcg(p.a + o);
+      c = row == p.N - 1 ? R(0) : __ldcg(p.c + o);
+      b = __ldcg(p.b + o);
+    } else {
+      a = row == 0 ? R(0) : R(__ldcg(cf.a + o));
+      c = row == p.N - 1 ? R(0) : R(__ldcg(cf.c + o));
+      b = R(__ldcg(cf.b + o));
+    }
     d = __ldcg(p.d_in + o);
   } else {
     a = R(0);
@@ -153,9 +164,10 @@ __device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, long long o
 
 }  // namespace
 
-template <typename R, int M, int D, bool INC>
+template <typename R, int M, int D, bool INC, typename CR = R>
 __global__ void __launch_bounds__(wide_bs<R>(), 1)
-    strided_wide_kernel(const BatchArgs<R> p, long long ngx, long long ngroups) {
+    strided_wide_kernel(const BatchArgs<R> p, const CoefPtrs<CR> cf, long long ngx, long long ngroups) {
+  static_assert(std::is_same<CR, R>::value || !INC, "the promoted form has no Inc");
   constexpr int W = wide_w<R>();
   constexpr int T = wide_t<R>();
   constexpr int BS = W * T;
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
   long long lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    wide_load_row<R, INC>(p, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
+    wide_load_row<R, CR>(p, cf, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
     lo += stride;
   }
 
@@ -224,11 +236,11 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
       const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
       if (j + D < M) {
         const int row = row0 + j + D;
-        wide_load_row<R, INC>(p, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        wide_load_row<R, CR>(p, cf, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
         lo += stride;
       } else {
         const int row = row0 + j + D - M;
-        wide_load_row<R, INC>(p, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
+        wide_load_row<R, CR>(p, cf, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
         ln += stride;
       }
       R af, cf, df;
@@ -345,8 +357,9 @@ template <typename R> int wide_rows_per_thread(int N) {
   return sizeof(R) == 4 && N <= 64 * T ? 64 : 0;
 }
 
-template <typename R, int M, bool INC>
-static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st) {
+template <typename R, int M, bool INC, typename CR = R>
+static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
+                                 const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
   constexpr int W = wide_w<R>();
   constexpr int T = wide_t<R>();
   constexpr int BS = W * T;
@@ -354,7 +367,7 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st) {
   const size_t red = ((size_t)6 * T * (W + 1) * sizeof(R) + 15) / 16 * 16;
   size_t smem = red + (size_t)M * BS * sizeof(R);
   if (smem < (size_t)WIDE_SMEM_MIN) smem = WIDE_SMEM_MIN;  // one CTA per SM
-  auto kern = strided_wide_kernel<R, M, D, INC>;
+  auto kern = strided_wide_kernel<R, M, D, INC, CR>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -363,7 +376,7 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long grid = ngroups < sms ? ngroups : sms;
-  kern<<<(unsigned)grid, BS, smem, st>>>(p, ngx, ngroups);
+  kern<<<(unsigned)grid, BS, smem, st>>>(p, cf, ngx, ngroups);
   return cudaGetLastError();
 }
 
@@ -376,6 +389,18 @@ cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st) {
     case 64:
       if constexpr (sizeof(R) == 4) return launch_wide_m<R, 64, INC>(p, st);
       return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Promoted solve: FP64 arithmetic on FP32-stored coefficients (cf), p.a,
+// p.b, p.c unused; 64 < N <= 512.
+cudaError_t launch_strided_wide_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
+                                         cudaStream_t st) {
+  switch (wide_rows_per_thread<double>(p.N)) {
+    case 8: return launch_wide_m<double, 8, false, float>(p, st, cf);
+    case 16: return launch_wide_m<double, 16, false, float>(p, st, cf);
+    case 32: return launch_wide_m<double, 32, false, float>(p, st, cf);
     default: return cudaErrorInvalidValue;
   }
 }
