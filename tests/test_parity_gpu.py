@@ -248,6 +248,9 @@ def test_contiguous_reciprocal_within_one_ulp(n, dt, emax):
     2^-emax to 2^emax of either sign. A zero pivot on the same path is still
     reported."""
     dims = [n, 64]
+    # the warp-per-system shared-memory kernel (FP32 systems of 256 rows
+    # take two per warp by default)
+    tb.force_plan(tb.FAMILY_HYBRID, n // 32)
     assert "smem" in tb.describe_plan(np.dtype(dt).itemsize, dims, 0)
     rng = np.random.default_rng(n)
     count = n * 64

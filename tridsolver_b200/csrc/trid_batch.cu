@@ -126,19 +126,24 @@ Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f) 
         const int fs = f.stream;
         const bool want_tma = f.tma == 1;
         const int fm = f.m;
-        // the wide form (256-byte groups, state in tensor memory) for FP64
-        // rows a whole plane apart (>= 64 KiB: z solves), where the rate of
-        // row segments limits 128-byte groups (512^3 z: 0.88 vs 1.11 ms, Inc
-        // 1.05 vs 1.47 ms), when at least half a group holds systems. Along y
-        // the 128-byte form with L2 prefetch measured faster (0.85 vs 0.87
-        // ms), and so did FP32 (whose 512-thread wide CTA has half the bytes
-        // in flight). Forced with tridForceStream(2) wherever it applies.
+        // the wide form (256-byte groups, state in tensor memory), when at
+        // least half a group holds systems, for
+        //  - rows a whole plane apart (>= 64 KiB: z solves), where the rate
+        //    of row segments limits 128-byte groups: FP64 512^3 z 0.89 vs
+        //    1.18 ms, Inc 1.04 vs 1.48 ms; FP32 systems over 256 rows 0.53
+        //    vs 0.61 ms, Inc 0.63 vs 0.81 ms (shorter FP32 systems measured
+        //    faster in 128-byte groups);
+        //  - FP64 Inc solves along y (256^3: 0.151 vs 0.165 ms; 512^3 equal).
+        // Along y without Inc the 128-byte form with L2 prefetch measured
+        // faster (FP64 0.857 vs 0.865 ms, FP32 0.51 vs 0.51 ms). Forced with
+        // tridForceStream(2) wherever it applies.
         const int mw = wide_rows_per_thread<R>(N);
         const bool zlike = p.stride * (long long)sizeof(R) >= (1LL << 16);
+        const bool wide_auto = sizeof(R) == 8 ? (zlike || p.u != nullptr) : (zlike && N > 256);
         if (mw > 0 && fm == 0 && !want_tma &&
-            (fs == 2 || (fs == -1 && sizeof(R) == 8 && zlike && 2 * p.n0 >= wide_width<R>()))) {
+            (fs == 2 || (fs == -1 && wide_auto && 2 * p.n0 >= wide_width<R>()))) {
           plan.M = mw;
-          plan.T = 512 / wide_width<R>();
+          plan.T = 16;  // chunks per system (one warp each)
           plan.W = wide_width<R>();
           plan.wide = true;
           return plan;

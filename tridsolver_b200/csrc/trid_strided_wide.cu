@@ -14,21 +14,31 @@
 //     columns of 32 bits per SM): the CTA allocates all 512 columns once,
 //     and each warp keeps its rows in its lane quarter (warp w: lanes
 //     32 (w % 4) .. + 31, columns (w / 4) * 128 .. + 127, i.e. 128 32-bit
-//     words per thread: 32 FP64 rows or 64 FP32 rows of a' and c');
-//   - d' goes to the thread's private shared-memory slots [j * BS + tid];
+//     words per thread: 32 rows of a' and c' of one FP64 system or of two
+//     FP32 systems);
+//   - d' goes to the thread's private shared-memory slots;
 //   - the chunk's top reduced row is accumulated in forward order during the
 //     forward sweep (x_1 = P + Q x_0 + S x_{k+1} as rows k are eliminated), so
 //     the parked state is read back once, by the back-substitution.
-// The CTA (512 threads; W systems x T chunks, thread (s, t) = (tid % W,
-// tid / W)) is persistent and walks over groups; each thread streams its
-// chunk's rows through a D-deep register window that runs on into the next
-// group, so loads stay in flight across the reduced solve and the stores.
+// The CTA (512 threads: 16 warps, warp t = chunk t of every system of the
+// group; lane l holds system l, and in FP32 also system l + 32, so a 64-
+// system FP32 group keeps the same bytes in flight as a 32-system FP64 one,
+// with two independent recurrences per thread) is persistent and walks over
+// groups; each thread streams its chunk's rows through a D-deep register
+// window that runs on into the next group, so loads stay in flight across
+// the reduced solve and the stores. The reduced systems are solved 32 at a
+// time (once per system of a thread).
 // The dynamic shared memory request is at least 120 KiB, so one CTA runs per
 // SM and the 512-column allocation never waits for another CTA of this
 // kernel. Every path through the kernel reaches the deallocation at its end.
 //
 // Inc variants load u block by block during the back-substitution (one
 // block ahead, the first block before the reduced solve).
+//
+// Pivots are inverted with the hardware reciprocal estimate (FP64: refined
+// by two Newton-Raphson steps), within one ulp of the correctly rounded
+// reciprocal, as in the contiguous kernels: measured equal in FP64 and a
+// little faster in FP32 (512^3 z Inc 0.658 -> 0.628 ms).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -41,11 +51,14 @@ namespace trid {
 namespace {
 
 template <typename R> constexpr int wide_w() { return 256 / (int)sizeof(R); }
-// chunks per system: 16 FP64 (32 systems x 16 = 512 threads), 8 FP32
-template <typename R> constexpr int wide_t() { return sizeof(R) == 8 ? 16 : 8; }
-template <typename R> constexpr int wide_bs() { return wide_w<R>() * wide_t<R>(); }
-// 32-bit TMEM columns per row: a' and c'
-template <typename R> constexpr int wide_cpr() { return 2 * (int)sizeof(R) / 4; }
+// systems per thread: 1 FP64, 2 FP32 (lanes l and l + 32 of a 64-system
+// group, two independent recurrences and the same bytes in flight)
+template <typename R> constexpr int wide_s() { return wide_w<R>() / 32; }
+// chunks per system (one warp each): 16, so 512 threads
+template <typename R> constexpr int wide_t() { return 16; }
+template <typename R> constexpr int wide_bs() { return 32 * wide_t<R>(); }
+// 32-bit TMEM columns per row: a' and c' of the thread's systems
+template <typename R> constexpr int wide_cpr() { return 2 * wide_s<R>() * (int)sizeof(R) / 4; }
 // rows per back-substitution block (one TMEM load of 32 columns; 16 for Inc)
 template <typename R, bool INC> constexpr int wide_blk() { return (INC ? 16 : 32) / wide_cpr<R>(); }
 constexpr int WIDE_SMEM_MIN = 120 * 1024;
@@ -70,17 +83,22 @@ __device__ __forceinline__ void tmem_fence_after_sync() {
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
 
-// one row's a', c' into this thread's lane at column `col`
-__device__ __forceinline__ void tmem_put_row(uint32_t taddr, double af, double cf) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr),
-               "r"(__double2loint(af)), "r"(__double2hiint(af)), "r"(__double2loint(cf)),
-               "r"(__double2hiint(cf))
-               : "memory");
-}
-__device__ __forceinline__ void tmem_put_row(uint32_t taddr, float af, float cf) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n" ::"r"(taddr), "r"(__float_as_uint(af)),
-               "r"(__float_as_uint(cf))
-               : "memory");
+// one row's a', c' (of the thread's S systems) into its lane at column taddr
+template <typename R, int S>
+__device__ __forceinline__ void tmem_put_row(uint32_t taddr, const R (&af)[S], const R (&cf)[S]) {
+  if constexpr (sizeof(R) == 8) {
+    static_assert(S == 1, "one FP64 system per thread");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr),
+                 "r"(__double2loint(af[0])), "r"(__double2hiint(af[0])), "r"(__double2loint(cf[0])),
+                 "r"(__double2hiint(cf[0]))
+                 : "memory");
+  } else {
+    static_assert(S == 2, "two FP32 systems per thread");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr),
+                 "r"(__float_as_uint(af[0])), "r"(__float_as_uint(cf[0])), "r"(__float_as_uint(af[1])),
+                 "r"(__float_as_uint(cf[1]))
+                 : "memory");
+  }
 }
 
 // 16 or 32 consecutive columns of this thread's lane (then tmem_wait_ld)
@@ -123,15 +141,15 @@ __device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[16]) {
                : "memory");
 }
 
-// a', c' of row i of a block loaded by tmem_get
-template <typename R, int NW>
-__device__ __forceinline__ void tmem_row(const uint32_t (&v)[NW], int i, R &af, R &cf) {
+// a', c' of row i, system q of a block loaded by tmem_get (4 columns a row)
+template <typename R, int S, int NW>
+__device__ __forceinline__ void tmem_row(const uint32_t (&v)[NW], int i, int q, R &af, R &cf) {
   if constexpr (sizeof(R) == 8) {
     af = __hiloint2double((int)v[4 * i + 1], (int)v[4 * i]);
     cf = __hiloint2double((int)v[4 * i + 3], (int)v[4 * i + 2]);
   } else {
-    af = __uint_as_float(v[2 * i]);
-    cf = __uint_as_float(v[2 * i + 1]);
+    af = __uint_as_float(v[4 * i + 2 * q]);
+    cf = __uint_as_float(v[4 * i + 2 * q + 1]);
   }
 }
 
@@ -166,29 +184,31 @@ __device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, const CoefP
 
 template <typename R, int M, int D, bool INC, typename CR = R>
 __global__ void __launch_bounds__(wide_bs<R>(), 1)
-    strided_wide_kernel(const BatchArgs<R> p, const CoefPtrs<CR> cf, long long ngx, long long ngroups) {
+    strided_wide_kernel(const BatchArgs<R> p, const CoefPtrs<CR> coef, long long ngx, long long ngroups) {
   static_assert(std::is_same<CR, R>::value || !INC, "the promoted form has no Inc");
-  constexpr int W = wide_w<R>();
+  constexpr int S = wide_s<R>();  // systems per thread: lanes l and l + 32 of the group
+  constexpr int W = wide_w<R>();  // = 32 * S
   constexpr int T = wide_t<R>();
-  constexpr int BS = W * T;
+  constexpr int BS = 32 * T;
   constexpr int NWARP = BS / 32;
   constexpr int CW = 512 / (NWARP / 4);  // TMEM columns per warp
-  constexpr int CPR = wide_cpr<R>();
+  constexpr int CPR = wide_cpr<R>();     // columns per row (a', c' of S systems)
   constexpr int B = wide_blk<R, INC>() < M ? wide_blk<R, INC>() : M;
   constexpr int NV = B * CPR;
   static_assert(NV == 16 || NV == 32, "one TMEM load per block");
   static_assert(NWARP % 4 == 0, "whole lane quarters");
   static_assert(M * CPR <= CW, "a' and c' of a chunk fit the warp's TMEM columns");
   static_assert(M % B == 0 && M % D == 0 && D <= M && M >= 4, "blocks and window tile the chunk");
-  constexpr int RED = (6 * T * (W + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
+  // reduced rows of one half-group (32 systems) at a time
+  constexpr int RED = (6 * T * 33 * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
   extern __shared__ __align__(16) unsigned char wide_smem[];
   __shared__ uint32_t tmem_slot;
   R *red = reinterpret_cast<R *>(wide_smem);
   const int tid = threadIdx.x;
-  R *sdf = red + RED + tid;  // d' of row j at [j * BS]
-  const int s = tid % W;
-  const int t = tid / W;
-  const int warp = tid >> 5;
+  R *sdf = red + RED + tid;  // d' of row j, system q at [(j * S + q) * BS]
+  const int lane = tid & 31;
+  const int t = tid >> 5;    // chunk = warp
+  const int warp = t;
   const int N = p.N;
   const int row0 = t * M;
   const long long stride = p.stride;
@@ -200,100 +220,131 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
   const uint32_t tbase = tmem_slot;
   const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * CW);
 
-  auto group_first = [&](long long g, bool &act) -> long long {
+  // element offset of system q's first chunk row in group g (0 if none)
+  auto group_first = [&](long long g, int q, bool &act) -> long long {
     const long long gx = g % ngx;
     const long long i1 = g / ngx;
-    const long long i0 = gx * W + s;
+    const long long i0 = gx * W + 32 * q + lane;
     act = g < ngroups && i0 < p.n0;
     return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
   };
 
-  R pa[D], pb[D], pc[D], pd[D];
+  R pa[S][D], pb[S][D], pc[S][D], pd[S][D];
   long long g = blockIdx.x;
-  bool act;
-  long long first = group_first(g, act);
-  long long lo = first;
+  bool act[S];
+  long long first[S], lo[S];
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    first[q] = group_first(g, q, act[q]);
+    lo[q] = first[q];
+  }
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    wide_load_row<R, CR>(p, cf, lo, act && row0 + j < N, row0 + j, pa[j], pb[j], pc[j], pd[j]);
-    lo += stride;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      wide_load_row<R, CR>(p, coef, lo[q], act[q] && row0 + j < N, row0 + j, pa[q][j], pb[q][j],
+                           pc[q][j], pd[q][j]);
+      lo[q] += stride;
+    }
   }
 
   bool bad = false;
   for (; g < ngroups; g += gridDim.x) {
-    bool actn;
-    const long long firstn = group_first(g + gridDim.x, actn);
-    long long ln = firstn;
+    bool actn[S];
+    long long firstn[S], ln[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      firstn[q] = group_first(g + gridDim.x, q, actn[q]);
+      ln[q] = firstn[q];
+    }
 
     // forward half of the chunk elimination, streamed row by row; the top
-    // reduced row accumulates as x_1 = P + Q x_0 + S x_{j+1}
-    R ap = R(0), cp = R(0), dp = R(0);
-    R a0 = R(0), c0 = R(0), d0 = R(0);
-    R P = R(0), Q = R(0), S = R(1);
+    // reduced row accumulates as x_1 = P + Q x_0 + Sg x_{j+1}
+    R ap[S], cp[S], dp[S], a0[S], c0[S], d0[S], P[S], Q[S], Sg[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      ap[q] = cp[q] = dp[q] = a0[q] = c0[q] = d0[q] = P[q] = Q[q] = R(0);
+      Sg[q] = R(1);
+    }
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int k = j % D;
-      const R a = pa[k], b = pb[k], c = pc[k], d = pd[k];
-      if (j + D < M) {
-        const int row = row0 + j + D;
-        wide_load_row<R, CR>(p, cf, lo, act && row < N, row, pa[k], pb[k], pc[k], pd[k]);
-        lo += stride;
-      } else {
-        const int row = row0 + j + D - M;
-        wide_load_row<R, CR>(p, cf, ln, actn && row < N, row, pa[k], pb[k], pc[k], pd[k]);
-        ln += stride;
+      R af[S], cfr[S];
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        const R a = pa[q][k], b = pb[q][k], c = pc[q][k], d = pd[q][k];
+        if (j + D < M) {
+          const int row = row0 + j + D;
+          wide_load_row<R, CR>(p, coef, lo[q], act[q] && row < N, row, pa[q][k], pb[q][k], pc[q][k],
+                               pd[q][k]);
+          lo[q] += stride;
+        } else {
+          const int row = row0 + j + D - M;
+          wide_load_row<R, CR>(p, coef, ln[q], actn[q] && row < N, row, pa[q][k], pb[q][k], pc[q][k],
+                               pd[q][k]);
+          ln[q] += stride;
+        }
+        R df;
+        if (j < 2) {
+          const R r = rcp_nr(b);
+          bad |= !finite_rcp(r);
+          af[q] = a * r;
+          cfr[q] = c * r;
+          df = d * r;
+        } else {
+          const R r = rcp_nr(b - a * cp[q]);
+          bad |= !finite_rcp(r);
+          df = r * (d - a * dp[q]);
+          af[q] = -r * a * ap[q];
+          cfr[q] = r * c;
+        }
+        sdf[(j * S + q) * BS] = df;
+        if (j == 0) {
+          a0[q] = af[q];
+          c0[q] = cfr[q];
+          d0[q] = df;
+        } else if (j <= M - 2) {
+          P[q] += Sg[q] * df;
+          Q[q] -= Sg[q] * af[q];
+          Sg[q] = -Sg[q] * cfr[q];
+        }
+        ap[q] = af[q];
+        cp[q] = cfr[q];
+        dp[q] = df;
       }
-      R af, cf, df;
-      if (j < 2) {
-        const R r = rcp(b);
-        bad |= !finite_rcp(r);
-        af = a * r;
-        cf = c * r;
-        df = d * r;
-      } else {
-        const R r = rcp(b - a * cp);
-        bad |= !finite_rcp(r);
-        df = r * (d - a * dp);
-        af = -r * a * ap;
-        cf = r * c;
-      }
-      tmem_put_row(taddr + (uint32_t)(j * CPR), af, cf);
-      sdf[j * BS] = df;
-      if (j == 0) {
-        a0 = af;
-        c0 = cf;
-        d0 = df;
-      } else if (j <= M - 2) {
-        P += S * df;
-        Q -= S * af;
-        S = -S * cf;
-      }
-      ap = af;
-      cp = cf;
-      dp = df;
+      tmem_put_row<R, S>(taddr + (uint32_t)(j * CPR), af, cfr);
     }
-    const R r0 = rcp(R(1) + c0 * Q);
-    bad |= !finite_rcp(r0);
-    const Row<R> top{r0 * a0, r0 * c0 * S, r0 * (d0 - c0 * P)};
-    const Row<R> bot{ap, cp, dp};
 
     // Inc: u of the last block, in flight during the reduced solve
-    long long o = first + (long long)(M - 1) * stride;
-    R ucur[INC ? B : 1], unext[INC ? B : 1];
-    if constexpr (INC) {
+    long long o[S];
+    R ucur[S][INC ? B : 1], unext[S][INC ? B : 1];
 #pragma unroll
-      for (int i = 0; i < B; ++i) {
-        const int j = M - 1 - i;
-        ucur[i] = (act && row0 + j < N) ? __ldcg(p.u + o - (long long)i * stride) : R(0);
+    for (int q = 0; q < S; ++q) {
+      o[q] = first[q] + (long long)(M - 1) * stride;
+      if constexpr (INC) {
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+          const int j = M - 1 - i;
+          ucur[q][i] = (act[q] && row0 + j < N) ? __ldcg(p.u + o[q] - (long long)i * stride) : R(0);
+        }
       }
     }
     tmem_wait_st();
-    R y, z;
-    block_reduced_solve<R, 2>(red, top, bot, s, t, T, W, y, z, bad);
+    R y[S], z[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      const R r0 = rcp(R(1) + c0[q] * Q[q]);
+      bad |= !finite_rcp(r0);
+      const Row<R> top{r0 * a0[q], r0 * c0[q] * Sg[q], r0 * (d0[q] - c0[q] * P[q])};
+      const Row<R> bot{ap[q], cp[q], dp[q]};
+      block_reduced_solve<R, 2>(red, top, bot, lane, t, T, 32, y[q], z[q], bad);
+    }
 
     // back-substitution with the parked rows, block by block from the
     // chunk's last row up, stored as it goes
-    R x = z;
+    R x[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) x[q] = z[q];
 #pragma unroll
     for (int bb = M / B - 1; bb >= 0; --bb) {
       uint32_t v[NV];
@@ -301,41 +352,52 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
       if constexpr (INC) {
         if (bb > 0) {
 #pragma unroll
-          for (int i = 0; i < B; ++i) {
-            const int j = bb * B - 1 - i;
-            unext[i] = (act && row0 + j < N) ? __ldcg(p.u + o - (long long)(B + i) * stride) : R(0);
-          }
+          for (int q = 0; q < S; ++q)
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+              const int j = bb * B - 1 - i;
+              unext[q][i] =
+                  (act[q] && row0 + j < N) ? __ldcg(p.u + o[q] - (long long)(B + i) * stride) : R(0);
+            }
         }
       }
       tmem_wait_ld(v);
 #pragma unroll
       for (int i = B - 1; i >= 0; --i) {
         const int j = bb * B + i;
-        if (j < M - 1) {
-          if (j == 0) {
-            x = y;
-          } else {
-            R af, cf;
-            tmem_row<R, NV>(v, i, af, cf);
-            x = sdf[j * BS] - af * y - cf * x;
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+          if (j < M - 1) {
+            if (j == 0) {
+              x[q] = y[q];
+            } else {
+              R af, cfq;
+              tmem_row<R, S, NV>(v, i, q, af, cfq);
+              x[q] = sdf[(j * S + q) * BS] - af * y[q] - cfq * x[q];
+            }
           }
+          if (act[q] && row0 + j < N) {
+            if constexpr (INC)
+              p.u[o[q]] = ucur[q][B - 1 - i] + x[q];
+            else
+              p.d_out[o[q]] = x[q];
+          }
+          o[q] -= stride;
         }
-        if (act && row0 + j < N) {
-          if constexpr (INC)
-            p.u[o] = ucur[B - 1 - i] + x;
-          else
-            p.d_out[o] = x;
-        }
-        o -= stride;
       }
       if constexpr (INC) {
 #pragma unroll
-        for (int i = 0; i < B; ++i) ucur[i] = unext[i];
+        for (int q = 0; q < S; ++q)
+#pragma unroll
+          for (int i = 0; i < B; ++i) ucur[q][i] = unext[q][i];
       }
     }
-    first = firstn;
-    act = actn;
-    lo = ln;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      first[q] = firstn[q];
+      act[q] = actn[q];
+      lo[q] = ln[q];
+    }
   }
   report_bad_pivot(bad, p.flag);
 
@@ -353,8 +415,7 @@ template <typename R> int wide_rows_per_thread(int N) {
   if (N <= 64 || N > 512) return 0;
   if (N <= 8 * T) return 8;
   if (N <= 16 * T) return 16;
-  if (N <= 32 * T) return 32;
-  return sizeof(R) == 4 && N <= 64 * T ? 64 : 0;
+  return N <= 32 * T ? 32 : 0;
 }
 
 template <typename R, int M, bool INC, typename CR = R>
@@ -362,10 +423,10 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
                                  const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
   constexpr int W = wide_w<R>();
   constexpr int T = wide_t<R>();
-  constexpr int BS = W * T;
+  constexpr int BS = 32 * T;
   constexpr int D = 4;
-  const size_t red = ((size_t)6 * T * (W + 1) * sizeof(R) + 15) / 16 * 16;
-  size_t smem = red + (size_t)M * BS * sizeof(R);
+  const size_t red = ((size_t)6 * T * 33 * sizeof(R) + 15) / 16 * 16;
+  size_t smem = red + (size_t)M * wide_s<R>() * BS * sizeof(R);
   if (smem < (size_t)WIDE_SMEM_MIN) smem = WIDE_SMEM_MIN;  // one CTA per SM
   auto kern = strided_wide_kernel<R, M, D, INC, CR>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -386,9 +447,6 @@ cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st) {
     case 8: return launch_wide_m<R, 8, INC>(p, st);
     case 16: return launch_wide_m<R, 16, INC>(p, st);
     case 32: return launch_wide_m<R, 32, INC>(p, st);
-    case 64:
-      if constexpr (sizeof(R) == 4) return launch_wide_m<R, 64, INC>(p, st);
-      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }
