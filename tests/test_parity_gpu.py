@@ -226,6 +226,21 @@ def test_long_systems(dims, solvedim, dt, oracle, reference):
     _check(dims, solvedim, dt, True, oracle, None, seed=5)
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("dims,solvedim,pads", [([513, 3], 0, None), ([1025, 2], 0, None),
+                                                ([1537, 5], 0, None), ([70001, 2], 0, None),
+                                                ([4097, 3, 2], 0, [4099, 3, 2]),
+                                                ([2048, 4], 0, [2051, 4]), ([600, 33], 0, None)])
+def test_long_contiguous_tiles(dims, solvedim, pads, inc, dt, oracle, reference):
+    """Long contiguous systems in warp tiles (two passes around the
+    second-level solve): partial last tiles, one to 137 tiles per system,
+    system starts off the 16-byte grid (odd padding), Inc."""
+    assert "tiles" in tb.describe_plan(np.dtype(dt).itemsize, dims, solvedim, pads) or \
+        dims[0] <= (512 if dt == np.float64 else 1024)
+    _check(dims, solvedim, dt, inc, oracle, reference if pads is None else None, pads=pads, seed=21)
+
+
 def test_zero_pivot_reported(oracle):
     a, b, c, d = make_system([16, 8], 0, np.float64)
     a[:] = 0.0

@@ -13,7 +13,8 @@ std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
   snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
-           smem ? " smem" : vec ? " vec" : tma ? " tma" : wide ? " wide" : streaming ? " stream" : "");
+           smem ? " smem" : vec ? " vec" : tma ? " tma" : wide ? " wide" : streaming ? " stream"
+           : tiles ? " tiles" : "");
   return buf;
 }
 
@@ -204,6 +205,9 @@ Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f) 
   }
   plan.family = TRID_FAMILY_LONG;
   plan.M = (M == 8 || M == 16) ? M : 16;
+  // contiguous systems: warp tiles staged by coalesced copies (trid_long.cu);
+  // strided ones: chunks of M rows per thread
+  plan.tiles = contig;
   return plan;
 }
 
@@ -353,6 +357,7 @@ cudaError_t launch_batch(const BatchArgs<R> &p, const Plan &plan, cudaStream_t s
   switch (plan.family) {
     case TRID_FAMILY_PCR: return launch_pcr<R, INC>(p, plan, st);
     case TRID_FAMILY_LONG:
+      if (plan.tiles) return launch_long_tiles<R, INC>(p, st);
       return plan.M == 8 ? launch_long_m<R, 8, INC>(p, st) : launch_long_m<R, 16, INC>(p, st);
     default:
       if (plan.wide) {

@@ -21,6 +21,7 @@ struct Plan {
   bool tma = false;                 // strided: TMA tiles, persistent, double-buffered
   bool streaming = false;           // strided: persistent streaming kernel (T = 32)
   bool wide = false;                // strided: wide streaming kernel (256-byte groups)
+  bool tiles = false;               // long, contiguous: warp tiles of 512 / 1024 rows
   std::string describe() const;
 };
 
@@ -130,6 +131,10 @@ template <typename R> int wide_rows_per_thread(int N);
 template <typename R> int wide_width();
 template <typename R, bool INC>
 cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st);
+// Long contiguous systems in warp tiles (trid_long.cu): reduction of every
+// tile to two second-level rows, recursive solve of those, substitution.
+template <typename R, bool INC>
+cudaError_t launch_long_tiles(const BatchArgs<R> &p, cudaStream_t st);
 // The wide kernel in FP64 arithmetic on FP32-stored a, b, c.
 cudaError_t launch_strided_wide_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
                                          cudaStream_t st);

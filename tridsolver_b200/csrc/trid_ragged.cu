@@ -37,17 +37,14 @@
 #include <mutex>
 
 #include "trid_internal.h"
+#include "trid_tile.cuh"
 #include "tridsolver_b200.h"
 
 namespace trid {
 
 constexpr int kClasses = 24;        // length classes 0..23: N <= 2^class
-// Tile items: rows per lane (16 FP64, 32 FP32: the same bytes, registers
-// and shared memory per tile), rows per tile (512 / 1024) and tiles per
-// system (N <= 16384 either way; the second-level system has at most 64
-// rows).
-template <typename R> constexpr int tile_m() { return sizeof(R) == 8 ? 16 : 32; }
-template <typename R> constexpr int tile_rows() { return 32 * tile_m<R>(); }
+// Tile items (tile_m / tile_rows, trid_tile.cuh): tiles per system, N <=
+// 16384 either way, so the second-level system has at most 64 rows.
 template <typename R> constexpr int max_tiles() { return 16384 / tile_rows<R>(); }
 constexpr int kRaggedThreads = 128; // 4 warps per CTA
 constexpr unsigned kWaitLimit = 1u << 22;  // polls of the ready flag (each with a short sleep)
@@ -194,126 +191,6 @@ __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base
   }
 }
 
-// The warp's reduced solve (as reduced_solve, 32 lanes) for three
-// right-hand sides sharing the matrix: k = 0 the rows' own D; k = 1 only
-// tD1 on the top row (lane 0: the coupling to the unknown before the
-// tile); k = 2 only bD2 on the bottom row (lane 31: the coupling to the one
-// after it).
-template <typename R>
-__device__ __forceinline__ void reduced_solve3(const Row<R> &top, const Row<R> &bot, R tD1, R bD2,
-                                               int t, R (&y)[3], R (&z)[3], bool &bad) {
-  constexpr int T = 32;
-  const R tD[3] = {top.D, tD1, R(0)};
-  const R bD[3] = {bot.D, R(0), bD2};
-  R pA = shfl_up(bot.A, 1, T), pC = shfl_up(bot.C, 1, T);
-  R de[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    R pD = shfl_up(bD[k], 1, T);
-    if (t == 0) pD = R(0);
-    de[k] = tD[k] - top.C * bD[k];
-    de[k] -= top.A * pD;
-  }
-  if (t == 0) {
-    pA = R(0);
-    pC = R(0);
-  }
-  R al = -top.A * pA;
-  const R be = R(1) - top.A * pC - top.C * bot.A;
-  R ga = -top.C * bot.C;
-  R r = rcp(be);
-  bad |= !finite_rcp(r);
-  al *= r;
-  ga *= r;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) de[k] *= r;
-#pragma unroll
-  for (int s = 1; s < T; s <<= 1) {
-    R al_l = shfl_up(al, s, T), ga_l = shfl_up(ga, s, T);
-    R al_r = shfl_down(al, s, T), ga_r = shfl_down(ga, s, T);
-    R dl[3], dr[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      dl[k] = shfl_up(de[k], s, T);
-      dr[k] = shfl_down(de[k], s, T);
-    }
-    if (t < s) {
-      al_l = ga_l = R(0);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) dl[k] = R(0);
-    }
-    if (t + s >= T) {
-      al_r = ga_r = R(0);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) dr[k] = R(0);
-    }
-    r = rcp(R(1) - al * ga_l - ga * al_r);
-    bad |= !finite_rcp(r);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) de[k] = (de[k] - al * dl[k] - ga * dr[k]) * r;
-    al = -al * al_l * r;
-    ga = -ga * ga_r * r;
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    y[k] = de[k];
-    R yn = shfl_down(y[k], 1, T);
-    if (t == T - 1) yn = R(0);
-    z[k] = bD[k] - bot.A * y[k] - bot.C * yn;
-  }
-}
-
-// Shared memory of one warp's tile: a, b, c, d in padded chunk rows (as
-// contig_smem_kernel), d's rows reused for x on the way out.
-template <typename R> struct TileBuf {
-  using L = SmemLayout<R, tile_m<R>()>;
-  static constexpr int ELEMS = 4 * L::BUF;
-  __device__ static __forceinline__ int slot(int e) { return (e / tile_m<R>()) * L::ROW + e % tile_m<R>(); }
-};
-
-// Copies rows [0, nt) of the tile starting at element `base` into the warp's
-// buffer and makes rows nt..511 identity rows. 16-byte cp.async units where
-// the tile's start is 16-byte aligned (each unit lies inside one lane's
-// chunk row, whose padded start is 16-byte aligned), element-sized copies
-// otherwise (32 consecutive elements per instruction) and for the tail.
-template <typename R>
-__device__ __forceinline__ void stage_tile(const RaggedArgs<R> &p, long long base, int nt, R *buf,
-                                           int lane) {
-  using L = SmemLayout<R, tile_m<R>()>;
-  constexpr int V = 16 / (int)sizeof(R);
-  int e0 = 0;
-  if (p.vec16 && base % V == 0) {
-    const int nfull = nt / V;
-#pragma unroll 4
-    for (int u = lane; u < nfull; u += 32) {
-      const int e = u * V;
-      const int o = TileBuf<R>::slot(e);
-      cp_async16(buf + 0 * L::BUF + o, p.a + base + e, 16);
-      cp_async16(buf + 1 * L::BUF + o, p.b + base + e, 16);
-      cp_async16(buf + 2 * L::BUF + o, p.c + base + e, 16);
-      cp_async16(buf + 3 * L::BUF + o, p.d + base + e, 16);
-    }
-    e0 = nfull * V;
-  }
-#pragma unroll 4
-  for (int e = e0 + lane; e < tile_rows<R>(); e += 32) {
-    const int o = TileBuf<R>::slot(e);
-    if (e < nt) {
-      cp_async_elem<R>(buf + 0 * L::BUF + o, p.a + base + e);
-      cp_async_elem<R>(buf + 1 * L::BUF + o, p.b + base + e);
-      cp_async_elem<R>(buf + 2 * L::BUF + o, p.c + base + e);
-      cp_async_elem<R>(buf + 3 * L::BUF + o, p.d + base + e);
-    } else {
-      buf[0 * L::BUF + o] = R(0);
-      buf[1 * L::BUF + o] = R(1);
-      buf[2 * L::BUF + o] = R(0);
-      buf[3 * L::BUF + o] = R(0);
-    }
-  }
-  cp_async_wait_all();
-  __syncwarp();
-}
-
 template <typename R>
 __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item, R *buf, int lane,
                                           bool &bad) {
@@ -327,7 +204,7 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
   const long long base0 = p.tile_base[item];
   const long long r0 = (long long)j * tile_rows<R>();
   const int nt = (int)(n - r0 < tile_rows<R>() ? n - r0 : tile_rows<R>());
-  stage_tile<R>(p, base0 + r0, nt, buf, lane);
+  stage_tile_rows<R>(p.a, p.b, p.c, p.d, p.vec16, base0 + r0, nt, buf, lane);
 
   constexpr int kTM = tile_m<R>();
   R a[kTM], b[kTM], c[kTM], d[kTM];
@@ -354,38 +231,15 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
     const R pl = shfl_idx(z[0], 31, 32), al = shfl_idx(z[1], 31, 32), bl = shfl_idx(z[2], 31, 32);
     bool last = false;
     if (lane == 0) {
-      // second-level rows:  top  A l_{j-1} + f + C l = D   (x_next eliminated)
-      //                     bot  A f + l + C f_{j+1} = D   (x_prev eliminated)
-      R tA, tC, tDv, bA, bC, bDv;
-      // bl == 0 (no coupling to x_next: then bf == 0 too) and af == 0 (none
-      // to x_prev: al == 0) reduce to the end-of-system forms
-      if (j == K - 1 || bl == R(0)) {
-        tA = -af;
-        tC = R(0);
-        tDv = pf;
-      } else {
-        const R q = bf / bl;
-        tA = -af + q * al;
-        tC = -q;
-        tDv = pf - q * pl;
-      }
-      if (j == 0 || af == R(0)) {
-        bA = R(0);
-        bC = -bl;
-        bDv = pl;
-      } else {
-        const R q = al / af;
-        bA = -q;
-        bC = q * bf - bl;
-        bDv = pl - q * pf;
-      }
+      Row<R> t2, b2;
+      second_level_rows<R>(pf, af, bf, pl, al, bl, j == 0, j == K - 1, t2, b2);
       R *tr = p.tile_rows + 6 * (ts + j);
-      tr[0] = tA;
-      tr[1] = tC;
-      tr[2] = tDv;
-      tr[3] = bA;
-      tr[4] = bC;
-      tr[5] = bDv;
+      tr[0] = t2.A;
+      tr[1] = t2.C;
+      tr[2] = t2.D;
+      tr[3] = b2.A;
+      tr[4] = b2.C;
+      tr[5] = b2.D;
       // release: the rows before the count; acquire: the other tiles' rows
       // for the warp that completes the count
       last = atomic_add_acq_rel(&p.sys_done[s], 1u) == (unsigned)(K - 1);
