@@ -171,16 +171,22 @@ if given is not None:
         off = pad_offset(pads)
         span = off + int(np.prod(pads))
 
-        def padded(v):
+        def padded(v, fill=3.0):
             # the whole padded extent from the interior pointer on: the
-            # reference's vectorised x sweep reads every padded row in full
-            # (pads[0] elements), beyond the last interior row's end
-            full = to_padded(v, dims, pads, fill=3.0)
-            return np.concatenate([full, np.full(max(0, span - full.size), 3.0, dt)])
+            # reference's vectorised x sweep (pads[0] a multiple of the SIMD
+            # width) reads every padded row in full, beyond the last interior
+            # row's end, and solves the padded rows as part of the system
+            # (pads[0] rows, not dims[0]). With c = 0 on the last interior row
+            # the interior does not depend on them, as long as they are a
+            # nonsingular continuation: a = c = 0 there, b = d = 3 (a = b =
+            # c = 3 gives a zero pivot on the second padded row, and its NaN
+            # reaches the interior through 0 * NaN)
+            full = to_padded(v, dims, pads, fill=fill)
+            return np.concatenate([full, np.full(max(0, span - full.size), fill, dt)])
 
         outs = []
         for lib in (restatement, reference):
-            arrs = [padded(v) for v in (a, b, c, d)]
+            arrs = [padded(v, f) for v, f in zip((a, b, c, d), (0.0, 3.0, 0.0, 3.0))]
             up = padded(u0) if inc else None
             lib.strided_batch(*(v[off:] for v in arrs), dims, solvedim, pads=pads,
                               u=up[off:] if inc else None)
