@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--only-config", default=None,
                     choices=["sweep", "adi", "adi_f32", "precision", "ragged", "adjoint", "dist",
-                             "long", "autotune"],
+                             "long", "autotune", "adi_backprop"],
                     help="run just one of the other configurations and print its JSON (profiling)")
     ap.add_argument("--ragged-systems", type=int, default=200000,
                     help="systems in the ragged configuration (200000 = the benchmark)")
@@ -766,25 +766,55 @@ def config_adjoint(dev, n=256, probes=1000):
             "bytes_floor_ratio": "9 words (a,b,c,w,x in; 4 gradients out) vs 5 for the forward solve"}
 
 
-def config_adi_backprop(dev, n=64, steps=50, every=10):
-    """50-step ADI run backpropagated to the initial field and to each step's
-    lambda, checkpointing every 10 steps."""
-    import time
+def config_adi_backprop(dev, hbm, n=256, steps=50, every=10):
+    """50-step FP64 ADI run on n^3 backpropagated to the initial field and to
+    each step's lambda, checkpointing every 10 steps (the forward pass keeps
+    every 10th field; the backward recomputes each segment, then runs the
+    native step adjoints). Timed with CUDA events against the forward run
+    alone. Words per point and step: forward 7 (fused step), recompute 7,
+    adjoint 51 (coefficient-array recompute 26, three transposed solves 15,
+    lambda reductions 6, stencil transpose 4)."""
     import torch
     from tridsolver_b200.adi import adi_run
+    stream = torch.cuda.current_stream()
     g = torch.Generator(device=dev).manual_seed(8)
-    u0 = torch.randn((n, n, n), generator=g, device=dev, dtype=torch.float64).requires_grad_(True)
-    lams = (0.1 + 0.9 * torch.rand(steps, generator=g, device=dev, dtype=torch.float64)).requires_grad_(True)
+    u0 = torch.randn((n, n, n), generator=g, device=dev, dtype=torch.float64)
+    lams = 0.1 + 0.9 * torch.rand(steps, generator=g, device=dev, dtype=torch.float64)
     w = torch.randn((n, n, n), generator=g, device=dev, dtype=torch.float64)
+
+    def fwd_only():
+        with torch.no_grad():
+            return adi_run(u0, lams, checkpoint_every=every)
+
+    def fwd_bwd():
+        u = u0.clone().requires_grad_(True)
+        lv = lams.clone().requires_grad_(True)
+        (w * adi_run(u, lv, checkpoint_every=every)).sum().backward()
+        return u, lv
+
+    fwd_only()
+    fwd_bwd()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loss = (w * adi_run(u0, lams, checkpoint_every=every)).sum()
-    loss.backward()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fwd_only()
+    e1.record(stream)
     torch.cuda.synchronize()
-    el = time.perf_counter() - t0
-    return {"grid": [n] * 3, "steps": steps, "checkpoint_every": every, "seconds": round(el, 3),
-            "grad_u0_finite": bool(torch.isfinite(u0.grad).all().item()),
-            "grad_lambda": [round(v, 6) for v in lams.grad[:5].tolist()]}
+    t_fwd = e0.elapsed_time(e1)
+    e0.record(stream)
+    u, lv = fwd_bwd()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_all = e0.elapsed_time(e1)
+    words = 7 + 7 + 51
+    gbs = words * 8 * n ** 3 * steps / t_all / 1e6
+    return {"grid": [n] * 3, "dtype": "f64", "steps": steps, "checkpoint_every": every,
+            "forward_ms_per_step": round(t_fwd / steps, 4),
+            "forward_backward_ms_per_step": round(t_all / steps, 4),
+            "backward_over_forward": round((t_all - t_fwd) / t_fwd, 2),
+            "words_per_point_step": words, "hbm_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
+            "grad_u0_finite": bool(torch.isfinite(u.grad).all().item()),
+            "grad_lambda": [round(v, 6) for v in lv.grad[:5].tolist()]}
 
 
 def run_configs(dev, hbm):
@@ -803,7 +833,7 @@ def run_configs(dev, hbm):
                      ("long_systems", lambda: config_long(dev, hbm)),
                      ("autotune", lambda: config_autotune(dev, hbm)),
                      ("dist_512_f64", lambda: config_dist(dev, hbm)),
-                     ("adi_backprop", lambda: config_adi_backprop(dev))):
+                     ("adi_backprop", lambda: config_adi_backprop(dev, hbm))):
         try:
             res[name] = fn()
         except Exception as e:  # keep the headline line whatever happens here
@@ -831,7 +861,8 @@ def main():
               "adjoint": lambda: config_adjoint(dev),
               "dist": lambda: config_dist(dev, hbm),
               "long": lambda: config_long(dev, hbm),
-              "autotune": lambda: config_autotune(dev, hbm)}[args.only_config]
+              "autotune": lambda: config_autotune(dev, hbm),
+              "adi_backprop": lambda: config_adi_backprop(dev, hbm)}[args.only_config]
         print(json.dumps({"config": args.only_config, "result": fn()}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -214,6 +214,23 @@ EXTERN_C tridStatus_t tridSADIStep(float *u, float *du, float *a, float *b, floa
                                    const float *lam, int *step, float alpha, int nx, int ny,
                                    int nz);
 
+/* Adjoint of one timestep of tridDADIStep / tridSADIStep (lambda = lam[0]:
+ * pass lam + k for the k-th step), for differentiating a multi-step run:
+ * given u (the step's input field, nx*ny*nz device array) and g = dL/du' (u'
+ * the step's output), writes ubar = dL/du (a separate array) and adds
+ * dL/dlambda to lambar[0] (a device scalar). The forward intermediates are
+ * recomputed from u (the coefficient-array form of the step), then the three
+ * transposed solves and the stencil transpose run, with the lambda
+ * derivative reduced in FP64 on the device; the scratch (seven arrays of the
+ * grid) comes from the library's pool. Edges up to 1024; no counterpart in
+ * the reference. */
+EXTERN_C tridStatus_t tridDADIStepAdjoint(const double *u, const double *g, double *ubar,
+                                          double *lambar, const double *lam, double alpha, int nx,
+                                          int ny, int nz);
+EXTERN_C tridStatus_t tridSADIStepAdjoint(const float *u, const float *g, float *ubar,
+                                          float *lambar, const float *lam, float alpha, int nx,
+                                          int ny, int nz);
+
 /* ---- adjoint ------------------------------------------------------------
  * No counterpart in the reference. For x = T^{-1} d solved along `solvedim`
  * (the forward call's arguments) and w = dL/dx, writes

@@ -5,9 +5,12 @@
   the x, y, z-Inc solves of adi_cpu.cpp:209-270), over several steps with
   per-step lambdas;
 * a CUDA graph of one timestep, replayed, equals eager steps exactly;
-* the differentiable torch timestep equals the native one, and its
-  gradients with respect to the initial field and every lambda match central
-  finite differences; checkpointing gives the same gradients.
+* the differentiable timestep (native forward, native adjoint) equals the
+  native one; its gradients with respect to the field and lambda equal those
+  of the same step written with torch ops over the differentiable solve
+  (the reference formulation below), and a multi-step run's gradients with
+  respect to the initial field and every lambda match central finite
+  differences; checkpointing gives the same gradients.
 """
 
 import numpy as np
@@ -17,6 +20,7 @@ import torch
 from helpers import normwise
 from oracle.pyoracle import Restatement
 from tridsolver_b200.adi import ADIHeat, adi_run, adi_step
+from tridsolver_b200.autograd import trid_solve
 
 pytestmark = pytest.mark.gpu
 
@@ -85,6 +89,40 @@ def test_graph_replay_equals_eager():
     torch.cuda.synchronize()
     assert int(graphed.step_counter.item()) == 11
     assert torch.equal(eager.u, graphed.u)
+
+
+def _torch_step(u, lam, alpha=1.0):
+    """The timestep with torch ops and the differentiable solve: the
+    reference formulation for the native adjoint (stencil, coefficient
+    arrays with identity boundary rows, x, y, z solves)."""
+    m = torch.zeros_like(u)
+    m[1:-1, 1:-1, 1:-1] = 1
+    a = -alpha * lam * m
+    b = 1 + 2 * alpha * lam * m
+    lap = torch.zeros_like(u)
+    lap[1:-1, 1:-1, 1:-1] = (u[:-2, 1:-1, 1:-1] + u[2:, 1:-1, 1:-1] + u[1:-1, :-2, 1:-1] +
+                             u[1:-1, 2:, 1:-1] + u[1:-1, 1:-1, :-2] + u[1:-1, 1:-1, 2:] -
+                             6 * u[1:-1, 1:-1, 1:-1])
+    du = lam * lap
+    du = trid_solve(a, b, a, du, dim=2)
+    du = trid_solve(a, b, a, du, dim=1)
+    return u + trid_solve(a, b, a, du, dim=0)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 2e-5)])
+@pytest.mark.parametrize("shape", [(12, 14, 16), (5, 40, 9), (33, 6, 70), (3, 3, 3)])
+@pytest.mark.parametrize("alpha", [1.0, 0.5])
+def test_native_adjoint_equals_torch_formulation(shape, dtype, tol, alpha):
+    u = torch.randn(shape, dtype=dtype, device="cuda")
+    w = torch.randn(shape, dtype=dtype, device="cuda")
+    grads = []
+    for step in (adi_step, _torch_step):
+        uu = u.clone().requires_grad_(True)
+        lam = torch.tensor(0.43, dtype=dtype, device="cuda", requires_grad=True)
+        (w * step(uu, lam, alpha)).sum().backward()
+        grads.append((uu.grad.cpu().numpy(), lam.grad.item()))
+    assert normwise(grads[0][0], grads[1][0]) <= tol
+    assert abs(grads[0][1] - grads[1][1]) <= tol * max(1.0, abs(grads[1][1])) * 10
 
 
 def test_torch_step_equals_native():

@@ -49,6 +49,8 @@ SYMBOLS = {
     "tridAutotune": (_I, [_I, _I, _I, _IP, _IP, _I, ctypes.POINTER(ctypes.c_float), ctypes.c_char_p,
                           _I]),
     "tridAutotuneReset": (_I, []),
+    "tridDADIStepAdjoint": (_I, [_P, _P, _P, _P, _P, ctypes.c_double, _I, _I, _I]),
+    "tridSADIStepAdjoint": (_I, [_P, _P, _P, _P, _P, ctypes.c_float, _I, _I, _I]),
     "tridDADIStep": (_I, [_P] * 7 + [ctypes.c_double, _I, _I, _I]),
     "tridSADIStep": (_I, [_P] * 7 + [ctypes.c_float, _I, _I, _I]),
     "tridDmtsvStridedBatchAdjoint": (_I, [_P] * 10 + [_I, _I, _IP, _IP]),

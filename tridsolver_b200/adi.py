@@ -12,11 +12,14 @@ u += z solve, with a = c = -alpha*lambda, b = 1 + 2*alpha*lambda.
   traffic per point); ``coefficient_arrays=True`` materialises a, b, c as the
   reference application does (a preprocessing kernel and three array solves,
   21 words per point).
-* ``adi_step`` / ``adi_run``: the same timestep written with torch ops and
-  the differentiable solve (tridsolver_b200.autograd), so a multi-step run
-  backpropagates to the initial field and to every step's lambda;
-  ``adi_run`` recomputes segments of ``checkpoint_every`` steps in the
-  backward pass instead of storing every intermediate field.
+* ``adi_step`` / ``adi_run``: the same timestep as a differentiable torch
+  function: forward is the native fused step, backward the native adjoint of
+  the step (tridDADIStepAdjoint / tridSADIStepAdjoint: the transposed solves,
+  the stencil transpose and the lambda derivative on the device), so a
+  multi-step run backpropagates to the initial field and to every step's
+  lambda with no torch arithmetic on the fields; ``adi_run`` recomputes
+  segments of ``checkpoint_every`` steps in the backward pass instead of
+  storing every intermediate field.
 
 Tensors are (nz, ny, nx), C-contiguous: x is the fastest dimension as in the
 reference.
@@ -28,7 +31,6 @@ import torch
 import torch.utils.checkpoint
 
 from . import _lib, api
-from .autograd import trid_solve
 
 
 class ADIHeat:
@@ -99,37 +101,55 @@ class ADIHeat:
 
 # ---- differentiable form --------------------------------------------------
 
-_masks = {}
+class ADIStep(torch.autograd.Function):
+    """One timestep u -> u' with lambda a 0-d tensor; both passes native."""
 
+    @staticmethod
+    def forward(ctx, u, lam, alpha):
+        if u.dim() != 3 or not u.is_cuda or u.dtype not in (torch.float32, torch.float64):
+            raise ValueError("u: CUDA tensor (nz, ny, nx) of float32 or float64")
+        u = u.contiguous()
+        lam = lam.detach().to(device=u.device, dtype=u.dtype).reshape(1).contiguous()
+        nz, ny, nx = u.shape
+        out = u.clone()
+        du = torch.empty_like(u)
+        lib = _lib.load()
+        f64 = u.dtype == torch.float64
+        fn = lib.tridDADIStep if f64 else lib.tridSADIStep
+        ct = ctypes.c_double if f64 else ctypes.c_float
+        with torch.cuda.device(u.device), api.on_stream(blocking=False):
+            st = fn(out.data_ptr(), du.data_ptr(), None, None, None, lam.data_ptr(), None,
+                    ct(alpha), nx, ny, nz)
+        if st != 0:
+            raise api.TridError(st, "ADI step")
+        ctx.save_for_backward(u, lam)
+        ctx.alpha = alpha
+        return out
 
-def _interior(shape, dtype, device):
-    key = (tuple(shape), dtype, device)
-    m = _masks.get(key)
-    if m is None:
-        m = torch.zeros(shape, dtype=dtype, device=device)
-        m[1:-1, 1:-1, 1:-1] = 1
-        _masks[key] = m
-    return m
-
-
-def adi_rhs(u, lam):
-    """lambda * (sum of the 6 neighbours - 6 u) inside, 0 on the boundary."""
-    lap = torch.zeros_like(u)
-    lap[1:-1, 1:-1, 1:-1] = (u[:-2, 1:-1, 1:-1] + u[2:, 1:-1, 1:-1] + u[1:-1, :-2, 1:-1] +
-                             u[1:-1, 2:, 1:-1] + u[1:-1, 1:-1, :-2] + u[1:-1, 1:-1, 2:] -
-                             6 * u[1:-1, 1:-1, 1:-1])
-    return lam * lap
+    @staticmethod
+    def backward(ctx, g):
+        u, lam = ctx.saved_tensors
+        g = g.contiguous()
+        nz, ny, nx = u.shape
+        ubar = torch.empty_like(u)
+        lambar = torch.zeros(1, dtype=u.dtype, device=u.device)
+        lib = _lib.load()
+        f64 = u.dtype == torch.float64
+        fn = lib.tridDADIStepAdjoint if f64 else lib.tridSADIStepAdjoint
+        ct = ctypes.c_double if f64 else ctypes.c_float
+        with torch.cuda.device(u.device), api.on_stream(blocking=False):
+            st = fn(u.data_ptr(), g.data_ptr(), ubar.data_ptr(), lambar.data_ptr(), lam.data_ptr(),
+                    ct(ctx.alpha), nx, ny, nz)
+        if st != 0:
+            raise api.TridError(st, "ADI step adjoint")
+        return ubar, (lambar.reshape(()) if ctx.needs_input_grad[1] else None), None
 
 
 def adi_step(u, lam, alpha=1.0):
     """One differentiable ADI timestep; lam is a 0-d tensor (may require grad)."""
-    m = _interior(u.shape, u.dtype, u.device)
-    a = -alpha * lam * m
-    b = 1 + 2 * alpha * lam * m
-    du = adi_rhs(u, lam)
-    du = trid_solve(a, b, a, du, dim=2)   # x
-    du = trid_solve(a, b, a, du, dim=1)   # y
-    return u + trid_solve(a, b, a, du, dim=0)  # z, added into u
+    if not torch.is_tensor(lam):
+        lam = torch.tensor(float(lam), dtype=u.dtype, device=u.device)
+    return ADIStep.apply(u, lam, alpha)
 
 
 def _segment(u, lams, alpha):

@@ -57,6 +57,25 @@ __global__ void __launch_bounds__(256) adi_preproc_kernel(const R *__restrict__ 
   }
 }
 
+template <typename R>
+cudaError_t launch_adi_preproc(const R *u, R *du, R *a, R *b, R *c, const R *lam, const int *step,
+                               R alpha, int nx, int ny, int nz, cudaStream_t st) {
+  const long long n = (long long)nx * ny * nz;
+  const int threads = 256;
+  long long blocks = (n + threads - 1) / threads;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  adi_preproc_kernel<R><<<(unsigned)blocks, threads, 0, st>>>(u, du, a, b, c, lam, step, alpha, nx, ny,
+                                                            nz);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+template cudaError_t launch_adi_preproc<double>(const double *, double *, double *, double *,
+                                                double *, const double *, const int *, double, int,
+                                                int, int, cudaStream_t);
+template cudaError_t launch_adi_preproc<float>(const float *, float *, float *, float *, float *,
+                                               const float *, const int *, float, int, int, int,
+                                               cudaStream_t);
+
 __global__ void adi_advance_kernel(int *step) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
@@ -108,13 +127,7 @@ static cudaError_t adi_arrays(R *u, R *du, R *a, R *b, R *c, const R *lam, int *
     b = scratch + n;
     c = scratch + 2 * n;
   }
-  const int threads = 256;
-  long long blocks = (n + threads - 1) / threads;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
-  adi_preproc_kernel<R><<<(unsigned)blocks, threads, 0, st>>>(u, du, a, b, c, lam, step, alpha, nx, ny,
-                                                            nz);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_adi_preproc<R>(u, du, a, b, c, lam, step, alpha, nx, ny, nz, st);
   const long long dims[3] = {nx, ny, nz};
   for (int sd = 0; sd < 3 && e == cudaSuccess; ++sd) {
     BatchArgs<R> p{};

@@ -143,6 +143,12 @@ template <int M>
 cudaError_t launch_strided_stream_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
                                            cudaStream_t st);
 
+// The ADI step's preprocessing kernel (trid_adi.cu): du = lambda L u on
+// interior points, 0 on the boundary, and one shared set of coefficient
+// arrays (identity rows on the boundary).
+template <typename R>
+cudaError_t launch_adi_preproc(const R *u, R *du, R *a, R *b, R *c, const R *lam, const int *step,
+                               R alpha, int nx, int ny, int nz, cudaStream_t st);
 // Solves of the fused ADI timestep (trid_adi_fused.cu): the x solve with the
 // 7-point stencil of u formed on the fly (du written), 1 <= nx <= 512; the y
 // or z solve of du in place (INC: u += solution), 1 <= N <= 512.
