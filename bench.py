@@ -808,7 +808,28 @@ def config_adi_backprop(dev, hbm, n=256, steps=50, every=10):
     t_all = e0.elapsed_time(e1)
     words = 7 + 7 + 51
     gbs = words * 8 * n ** 3 * steps / t_all / 1e6
+    # central finite differences of the loss: 3 lambdas (h = 1e-5) and 3
+    # entries of the initial field (the run is linear in u0, so h = 1 is
+    # exact up to rounding)
+    fd = []
+    with torch.no_grad():
+        def loss(uu, lvv):
+            return (w * adi_run(uu, lvv, checkpoint_every=0)).sum().item()
+        for k in (0, steps // 2, steps - 1):
+            h = 1e-5
+            lp, lm = lams.clone(), lams.clone()
+            lp[k] += h
+            lm[k] -= h
+            est = (loss(u0, lp) - loss(u0, lm)) / (2 * h)
+            fd.append(abs(est - lv.grad[k].item()) / max(1.0, abs(est)))
+        for idx in ((1, 1, 1), (n // 2, n // 3, n // 4), (n - 2, 7, n // 2)):
+            up, um = u0.clone(), u0.clone()
+            up[idx] += 1.0
+            um[idx] -= 1.0
+            est = (loss(up, lams) - loss(um, lams)) / 2.0
+            fd.append(abs(est - u.grad[idx].item()) / max(1.0, abs(est)))
     return {"grid": [n] * 3, "dtype": "f64", "steps": steps, "checkpoint_every": every,
+            "fd_probes": len(fd), "fd_worst_rel_error": max(fd),
             "forward_ms_per_step": round(t_fwd / steps, 4),
             "forward_backward_ms_per_step": round(t_all / steps, 4),
             "backward_over_forward": round((t_all - t_fwd) / t_fwd, 2),

@@ -15,8 +15,8 @@
 // (T = 1 is thread-per-system Thomas, T = 32 a warp per system; strided
 // batches up to 128 chunks, a block per system); for strided batches the
 // register-tile kernel, the 128-byte and the wide (256-byte) streaming
-// kernels and TMA tiles; and the long multi-block path. Ties keep the
-// built-in choice. Later automatic plan choices for the same class on this
+// kernels and TMA tiles; and the long multi-block path. Candidates within
+// 3% of the built-in choice keep it. Later automatic plan choices for the same class on this
 // device use the recorded recipe; tridForce* settings still take
 // precedence, and tridAutotuneReset forgets the recipes.
 #include <cuda_runtime.h>
@@ -180,8 +180,9 @@ tridStatus_t autotune_shape(int ndim, int solvedim, const int *dims, const int *
       ms /= reps;
       if (round == 0) reps = ms > 0.f ? (int)fminf(200.f, fmaxf(3.f, 20.f / ms)) : 3;
     }
-    // ties (within 1%) keep the earlier candidate, the built-in choice first
-    if (ms > 0.f && ms < 0.99f * best) {
+    // near-ties (within 3%, about the run-to-run spread of these timings)
+    // keep the earlier candidate, the built-in choice first
+    if (ms > 0.f && ms < 0.97f * best) {
       best = ms;
       best_f = f;
       best_d = desc;
