@@ -575,7 +575,16 @@ def config_precision(dev, n=512, dims=None):
                                                                12, 1e-12), 5, stream)
             tm = _timed(lambda: tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, w, 3, axis, dims,
                                                               dims, 12, 1e-12), 5, stream)
+            # the FP32-values form with its refinement forced (mode 1)
+            tb.set_mixed_mode(1)
+            tmr = _timed(lambda: tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, w, 3, axis, dims,
+                                                               dims, 12, 1e-12), 5, stream)
             tb.set_blocking(True)
+            xmr = d.clone()
+            _, it_mr, _ = tb.tridDmtsvStridedBatchMixed(None, a32, b32, c32, xmr, 3, axis, dims, dims,
+                                                        12, 1e-12)
+            err_mr = rel(xmr, xp)
+            tb.set_mixed_mode(0)
             out.append({
                 "margin_min": 10.0 ** lo, "axis": "xyz"[axis], "fp64_ms": round(t64, 4),
                 "refine_fp64_system": {
@@ -588,9 +597,12 @@ def config_precision(dev, n=512, dims=None):
                     "strategy": "refinement" if it_m else "direct FP64 solve of the FP32 values",
                     "max_rel_error_vs_fp64_of_fp32_values": err_m_own,
                     "max_rel_error_vs_fp64_system": err_m_64, "ms": round(tm, 4),
-                    "time_over_fp64": round(tm / t64, 3), "bytes_per_element": 28},
+                    "time_over_fp64": round(tm / t64, 3), "bytes_per_element": 28,
+                    "refinement_forced": {"ms": round(tmr, 4), "time_over_fp64": round(tmr / t64, 3),
+                                          "iterations": it_mr,
+                                          "max_rel_error_vs_fp64_of_fp32_values": err_mr}},
             })
-            del x64, xr, xp, xm, w
+            del x64, xr, xp, xm, xmr, w
         del a32, b32, c32, a, b, c, d
         torch.cuda.empty_cache()
     return out

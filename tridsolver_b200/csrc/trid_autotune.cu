@@ -15,10 +15,12 @@
 // (T = 1 is thread-per-system Thomas, T = 32 a warp per system; strided
 // batches up to 128 chunks, a block per system); for strided batches the
 // register-tile kernel, the 128-byte and the wide (256-byte) streaming
-// kernels and TMA tiles; and the long multi-block path. Candidates within
-// 3% of the built-in choice keep it. Later automatic plan choices for the same class on this
-// device use the recorded recipe; tridForce* settings still take
-// precedence, and tridAutotuneReset forgets the recipes.
+// kernels and TMA tiles; and the long multi-block path. A candidate must
+// beat the best so far by 3% (about the run-to-run spread of the timings),
+// so near-ties keep the built-in choice. Later automatic plan choices for
+// the same class on this device use the recorded recipe; tridForce*
+// settings still take precedence, and tridAutotuneReset forgets the
+// recipes.
 #include <cuda_runtime.h>
 
 #include <cmath>
