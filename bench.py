@@ -783,9 +783,9 @@ def config_adi_backprop(dev, hbm, n=256, steps=50, every=10):
     each step's lambda, checkpointing every 10 steps (the forward pass keeps
     every 10th field; the backward recomputes each segment, then runs the
     native step adjoints). Timed with CUDA events against the forward run
-    alone. Words per point and step: forward 7 (fused step), recompute 7,
-    adjoint 51 (coefficient-array recompute 26, three transposed solves 15,
-    lambda reductions 6, stencil transpose 4)."""
+    alone. Words per point and step: forward 7 (fused step), segment
+    recompute 7, adjoint 28 (forward intermediates 10, copy of the gradient
+    2, three transposed solves 6, lambda reductions 6, stencil transpose 4)."""
     import torch
     from tridsolver_b200.adi import adi_run
     stream = torch.cuda.current_stream()
@@ -818,7 +818,7 @@ def config_adi_backprop(dev, hbm, n=256, steps=50, every=10):
     e1.record(stream)
     torch.cuda.synchronize()
     t_all = e0.elapsed_time(e1)
-    words = 7 + 7 + 51
+    words = 7 + 7 + 28
     gbs = words * 8 * n ** 3 * steps / t_all / 1e6
     # central finite differences of the loss: 3 lambdas (h = 1e-5) and 3
     # entries of the initial field (the run is linear in u0, so h = 1 is

@@ -110,7 +110,10 @@ def _torch_step(u, lam, alpha=1.0):
 
 
 @pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 2e-5)])
-@pytest.mark.parametrize("shape", [(12, 14, 16), (5, 40, 9), (33, 6, 70), (3, 3, 3)])
+@pytest.mark.parametrize("shape", [(12, 14, 16), (5, 40, 9), (33, 6, 70), (3, 3, 3), (2, 7, 5),
+                                   (130, 4, 3), (20, 300, 17),
+                                   # an edge over 512: the coefficient-array form
+                                   (4, 3, 600)])
 @pytest.mark.parametrize("alpha", [1.0, 0.5])
 def test_native_adjoint_equals_torch_formulation(shape, dtype, tol, alpha):
     u = torch.randn(shape, dtype=dtype, device="cuda")

@@ -407,10 +407,14 @@ template <typename R, int T> constexpr int adi_bs() { return T * adi_w<R>(); }
 // Work: the (tile, plane) steps, tile-major, are split evenly over the grid
 // (one CTA per SM); a CTA whose range crosses into the next tile restarts
 // its ring there.
-template <typename R, int M, bool VEC, int J, int LA>
+// TRANS: the transposed solve of the step's x matrix in place (u == du):
+// the right-hand side is the line itself with rows 0 and nx - 1 taken as 0,
+// boundary lines and rows 0, nx - 1 are not stored (see launch_adi_x_transposed).
+template <typename R, int M, bool VEC, int J, int LA, bool TRANS = false>
 __global__ void __launch_bounds__(J * 16, 1)
-    adi_x_kernel(const R *__restrict__ u, R *__restrict__ du, const ConstCoef<R> k, unsigned *flag,
-                 int nx, int ny, int nz, int jtiles) {
+    adi_x_kernel(const R *u, R *du, const ConstCoef<R> k, unsigned *flag, int nx, int ny, int nz,
+                 int jtiles) {
+  static_assert(!(TRANS && VEC), "the transposed form stores element by element");
   static_assert(J % 2 == 0, "two lines per warp");
   using S = SwzLine<R, M>;
   constexpr int LB = S::LEN;           // elements per line buffer
@@ -517,9 +521,33 @@ __global__ void __launch_bounds__(J * 16, 1)
         const bool z1 = kbnd || j + 1 == ny - 1;
         const bool has1 = j + 1 < ny;
         if (z0 && (z1 || !has1)) {
-          store_line(dst, outb, true);
-          if (has1) store_line(dst + nx, outb, true);
+          if constexpr (!TRANS) {
+            store_line(dst, outb, true);
+            if (has1) store_line(dst + nx, outb, true);
+          }
           have = false;
+        } else if constexpr (TRANS) {
+          // the lines themselves as right-hand sides, rows 0 and nx - 1 as 0
+          const R *sc = ring + ((kz - kb + 1) % NS) * SL * LB;
+          R d0[M], d1[M];
+          lds_swz<R, M>(sc + (2 * warp + 1) * LB, lane, d0);
+          lds_swz<R, M>(sc + (2 * warp + 2) * LB, lane, d1);
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            const int row = lane * M + i;
+            const bool in = row >= 1 && row <= nx - 2;
+            d0[i] = in ? d0[i] : R(0);
+            d1[i] = in ? d1[i] : R(0);
+          }
+          contig_solve_d2<R, M>(f, d0, d1, lane, cl);
+          sts_swz<R, M>(outb, lane, d0);
+          sts_swz<R, M>(outb + LB, lane, d1);
+          __syncwarp();
+          // interior rows of interior lines only
+          for (int e = 1 + lane; e < nx - 1; e += 32) {
+            if (!z0) dst[e] = outb[S::idx(e)];
+            if (has1 && !z1) dst[nx + e] = outb[LB + S::idx(e)];
+          }
         } else {
           // slab line w2 + 1 holds line j (line 0 of the slab is j0 - 1)
           const int w2 = 2 * warp;
@@ -602,9 +630,13 @@ __global__ void __launch_bounds__(J * 16, 1)
 // through the window and parked in private shared-memory slots until the
 // store.
 // O32: element offsets in 32 bits (the launcher's choice when they fit).
-template <typename R, int M, int D, int PF, bool INC, int T, bool O32 = false>
+// TRANS: the transposed solve in place (p.d_in == p.d_out): rows 0 and N - 1
+// of the interior systems enter as 0 and are not stored (see
+// launch_adi_yz_transposed).
+template <typename R, int M, int D, int PF, bool INC, int T, bool O32 = false, bool TRANS = false>
 __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
     adi_stream_kernel(const BatchArgs<R> p, const ConstCoef<R> k, long long ngx, long long ngroups) {
+  static_assert(!(TRANS && INC), "the transposed form overwrites");
   static_assert(M >= 4 && D >= 1 && D <= M && M % D == 0, "window must tile the chunk");
   static_assert(PF == 0 || (PF > D && PF <= M), "L2 prefetch runs ahead of the window");
   constexpr int W = adi_w<R>();
@@ -701,7 +733,7 @@ __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
   IX lo = first;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    const bool v = act && row0 + j < N;
+    const bool v = act && row0 + j < N && !(TRANS && (row0 + j == 0 || row0 + j == N - 1));
     pd[j] = v ? __ldg(p.d_in + lo) : R(0);
     if constexpr (INC) pu[j] = v ? __ldg(p.u + lo) : R(0);
     lo += stride;
@@ -730,7 +762,7 @@ __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
       {
         const bool nxt = j + D >= M;
         const int row = nxt ? row0 + j + D - M : row0 + j + D;
-        const bool v = (nxt ? actn : act) && row < N;
+        const bool v = (nxt ? actn : act) && row < N && !(TRANS && (row == 0 || row == N - 1));
         const IX o = nxt ? ln : lo;
         pd[kk] = v ? __ldg(p.d_in + o) : R(0);
         if constexpr (INC) pu[kk] = v ? __ldg(p.u + o) : R(0);
@@ -789,7 +821,7 @@ __global__ void __launch_bounds__(adi_bs<R, T>(), adi_ctas_per_sm<R, M, T>())
         const Pair<R> ac = f.acf[j][t];
         x = j == 0 ? y : rd[j] - ac.x * y - ac.y * x;
       }
-      if (act && row0 + j < N) {
+      if (act && row0 + j < N && !(TRANS && (row0 + j == 0 || row0 + j == N - 1))) {
         if constexpr (INC)
           p.u[o] = suf[j * BS] + x;
         else
@@ -818,11 +850,11 @@ static constexpr size_t adi_x_smem() {
          (size_t)((LA + 3) * (J + 2) + J) * SwzLine<R, M>::LEN * sizeof(R);
 }
 
-template <typename R, int M, bool VEC, int J, int LA>
+template <typename R, int M, bool VEC, int J, int LA, bool TRANS = false>
 static cudaError_t launch_adi_x_j(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
                                   int ny, int nz, cudaStream_t st) {
   const size_t smem = adi_x_smem<R, M, VEC, J, LA>();
-  auto kern = adi_x_kernel<R, M, VEC, J, LA>;
+  auto kern = adi_x_kernel<R, M, VEC, J, LA, TRANS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
@@ -841,13 +873,13 @@ static cudaError_t launch_adi_x_j(const R *u, R *du, const ConstCoef<R> &k, unsi
 
 // Tile of 16 lines with slabs one plane ahead where it fits in shared
 // memory, else 8 lines.
-template <typename R, int M, bool VEC>
+template <typename R, int M, bool VEC, bool TRANS = false>
 static cudaError_t launch_adi_x_mv(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
                                    int ny, int nz, cudaStream_t st) {
   if constexpr (adi_x_smem<R, M, VEC, 16, 1>() <= 224 * 1024)
-    return launch_adi_x_j<R, M, VEC, 16, 1>(u, du, k, flag, nx, ny, nz, st);
+    return launch_adi_x_j<R, M, VEC, 16, 1, TRANS>(u, du, k, flag, nx, ny, nz, st);
   else
-    return launch_adi_x_j<R, M, VEC, 8, 1>(u, du, k, flag, nx, ny, nz, st);
+    return launch_adi_x_j<R, M, VEC, 8, 1, TRANS>(u, du, k, flag, nx, ny, nz, st);
 }
 
 template <typename R>
@@ -863,10 +895,24 @@ cudaError_t launch_adi_x(const R *u, R *du, const ConstCoef<R> &k, unsigned *fla
              : launch_adi_x_mv<R, 16, false>(u, du, k, flag, nx, ny, nz, st);
 }
 
+// The transposed solve of the step's x matrix, in place on w (1 <= nx <=
+// 512). The matrix has identity rows on the boundary and constant interior
+// rows, so its transpose's interior block is its own: the interior of every
+// interior line is the solve of that line's interior (rows 0 and nx - 1 as
+// 0), and boundary lines and rows are left as they are (adi_transposed_fixup
+// then adds the one coupling of rows 0 and nx - 1).
+template <typename R>
+cudaError_t launch_adi_x_transposed(R *w, const ConstCoef<R> &k, int nx, int ny, int nz,
+                                    cudaStream_t st) {
+  if (nx < 1 || nx > 512 || ny < 1 || nz < 1) return cudaErrorInvalidValue;
+  if (nx <= 256) return launch_adi_x_mv<R, 8, false, true>(w, w, k, nullptr, nx, ny, nz, st);
+  return launch_adi_x_mv<R, 16, false, true>(w, w, k, nullptr, nx, ny, nz, st);
+}
+
 template <typename R, int M> constexpr int adi_window() { return M < 8 ? M : 8; }
 template <typename R, int M> constexpr int adi_prefetch() { return adi_window<R, M>() >= M ? 0 : 12; }
 
-template <typename R, int M, int T, int PF, bool INC>
+template <typename R, int M, int T, int PF, bool INC, bool TRANS = false>
 static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   constexpr int W = adi_w<R>();
   constexpr int BS = adi_bs<R, T>();
@@ -879,9 +925,9 @@ static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R
   // 2% faster per timestep there, no gain in FP32)
   const long long maxoff = (p.n0 - 1) * p.st0 + (p.nsys / p.n0 - 1) * p.st1 + (long long)(p.N - 1) * p.stride;
   const bool o32 = maxoff < (1LL << 31) - 1 - 64LL * p.stride;
-  auto kern = adi_stream_kernel<R, M, D, PF, INC, T, false>;
+  auto kern = adi_stream_kernel<R, M, D, PF, INC, T, false, TRANS>;
   if constexpr (sizeof(R) == 8) {
-    if (o32) kern = adi_stream_kernel<R, M, D, PF, INC, T, true>;
+    if (o32) kern = adi_stream_kernel<R, M, D, PF, INC, T, true, TRANS>;
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -898,12 +944,12 @@ static cudaError_t launch_adi_stream_pf(const BatchArgs<R> &p, const ConstCoef<R
   return cudaGetLastError();
 }
 
-template <typename R, int M, int T, bool INC>
+template <typename R, int M, int T, bool INC, bool TRANS = false>
 static cudaError_t launch_adi_stream_m(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
   constexpr int PF = adi_prefetch<R, M>();
   if (PF > 0 && p.stride * (long long)sizeof(R) < (1LL << 16))
-    return launch_adi_stream_pf<R, M, T, PF, INC>(p, k, st);
-  return launch_adi_stream_pf<R, M, T, 0, INC>(p, k, st);
+    return launch_adi_stream_pf<R, M, T, PF, INC, TRANS>(p, k, st);
+  return launch_adi_stream_pf<R, M, T, 0, INC, TRANS>(p, k, st);
 }
 
 // y or z solve of the timestep: p.d_in == p.d_out == du, p.u = u for the z
@@ -926,6 +972,34 @@ cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStre
   }
 }
 
+// The transposed y or z solve of the step, in place on p.d_in == p.d_out
+// (1 <= N <= 512): interior systems get the solve of their interior rows
+// (rows 0 and N - 1 as 0, not stored), boundary systems are left as they
+// are (see launch_adi_x_transposed).
+template <typename R>
+cudaError_t launch_adi_yz_transposed(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st) {
+  if (p.N < 1 || p.N > 512 || p.n0 < 1 || p.nsys % p.n0 || p.d_in != p.d_out) return cudaErrorInvalidValue;
+  if (p.n0 >= (1LL << 31) || p.nsys / p.n0 >= (1LL << 31)) return cudaErrorInvalidValue;
+  if (p.nsys == 0) return cudaSuccess;
+  if constexpr (sizeof(R) == 4) {
+    if (p.N <= 128) return launch_adi_stream_m<R, 8, 16, false, true>(p, k, st);
+    if (p.N <= 256) return launch_adi_stream_m<R, 16, 16, false, true>(p, k, st);
+    return launch_adi_stream_m<R, 16, 32, false, true>(p, k, st);
+  } else {
+    if (p.N <= 128) return launch_adi_stream_m<R, 4, 32, false, true>(p, k, st);
+    if (p.N <= 256) return launch_adi_stream_m<R, 8, 32, false, true>(p, k, st);
+    return launch_adi_stream_m<R, 16, 32, false, true>(p, k, st);
+  }
+}
+
+template cudaError_t launch_adi_x_transposed<double>(double *, const ConstCoef<double> &, int, int, int,
+                                                     cudaStream_t);
+template cudaError_t launch_adi_x_transposed<float>(float *, const ConstCoef<float> &, int, int, int,
+                                                    cudaStream_t);
+template cudaError_t launch_adi_yz_transposed<double>(const BatchArgs<double> &,
+                                                      const ConstCoef<double> &, cudaStream_t);
+template cudaError_t launch_adi_yz_transposed<float>(const BatchArgs<float> &, const ConstCoef<float> &,
+                                                     cudaStream_t);
 template cudaError_t launch_adi_x<double>(const double *, double *, const ConstCoef<double> &,
                                           unsigned *, int, int, int, cudaStream_t);
 template cudaError_t launch_adi_x<float>(const float *, float *, const ConstCoef<float> &, unsigned *,

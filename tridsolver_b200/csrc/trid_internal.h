@@ -157,6 +157,14 @@ cudaError_t launch_adi_x(const R *u, R *du, const ConstCoef<R> &k, unsigned *fla
                          int nz, cudaStream_t st);
 template <typename R, bool INC>
 cudaError_t launch_adi_yz(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st);
+// Transposed solves of the step's matrices, in place (the step's adjoint):
+// interior rows of interior systems solved, rows 0 and N - 1 and boundary
+// systems left as they are (1 <= N <= 512).
+template <typename R>
+cudaError_t launch_adi_x_transposed(R *w, const ConstCoef<R> &k, int nx, int ny, int nz,
+                                    cudaStream_t st);
+template <typename R>
+cudaError_t launch_adi_yz_transposed(const BatchArgs<R> &p, const ConstCoef<R> &k, cudaStream_t st);
 
 // Distributed solve (trid_dist.cu): whether ctx->mpi_params was registered
 // by tridDistInit, and the solve of this rank's block.
