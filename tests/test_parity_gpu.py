@@ -200,6 +200,39 @@ def test_tma_tiles(dims, solvedim, tma, inc, dt, oracle, reference):
         tb.force_tma(-1)
 
 
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("offset", [0, 2, 1])
+@pytest.mark.parametrize("dims,solvedim", [([64, 7, 100], 2), ([128, 3, 200], 2), ([64, 300, 3], 1),
+                                           ([128, 5, 511], 2), ([64, 257], 1), ([192, 66], 1),
+                                           ([64, 2, 256], 2), ([64, 129, 2], 1)])
+def test_wide_pairs(dims, solvedim, inc, offset, oracle, reference):
+    """FP32 wide kernel in the paired form (two adjacent systems a thread,
+    8-byte accesses): every chunk count and size (8 x 16, 8 x 32, 16 x 32
+    rows), lengths that end inside a chunk; an odd offset (arrays not 8-byte
+    aligned) takes the unpaired form."""
+    tb.force_stream(2)
+    try:
+        _check(dims, solvedim, np.float32, inc, oracle, reference, offset=offset,
+               seed=11 + offset + 2 * inc + solvedim)
+    finally:
+        tb.force_stream(-1)
+
+
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("dims,pads,solvedim", [([64, 30, 100], [66, 32, 100], 2),
+                                                ([64, 30, 100], [65, 31, 100], 2),
+                                                ([128, 150, 3], [130, 150, 3], 1)])
+def test_wide_pairs_padded(dims, pads, solvedim, inc, oracle, reference):
+    """Padded FP32 batches in the wide kernel. In the reference's layout the
+    arrays start at element (1, 1, 1) of the padded grid, an odd offset for
+    any pads that keep the strides even, so these take the unpaired form."""
+    tb.force_stream(2)
+    try:
+        _check(dims, solvedim, np.float32, inc, oracle, reference, pads=pads, seed=21 + 2 * inc)
+    finally:
+        tb.force_stream(-1)
+
+
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 @pytest.mark.parametrize("inc", [False, True])
 @pytest.mark.parametrize("stream", [2, 1, 0])

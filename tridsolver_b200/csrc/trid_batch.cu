@@ -13,8 +13,8 @@ std::string Plan::describe() const {
   char buf[96];
   const char *fam = family == TRID_FAMILY_PCR ? "pcr" : family == TRID_FAMILY_LONG ? "long" : "hybrid";
   snprintf(buf, sizeof(buf), "%s M=%d T=%d W=%d%s", fam, M, T, W,
-           smem ? " smem" : vec ? " vec" : tma ? " tma" : wide ? " wide" : streaming ? " stream"
-           : tiles ? " tiles" : "");
+           smem ? " smem" : vec ? " vec" : tma ? " tma" : wide ? (pairs ? " wide pairs" : " wide")
+           : streaming ? " stream" : tiles ? " tiles" : "");
   return buf;
 }
 
@@ -130,23 +130,35 @@ Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f) 
         // the wide form (256-byte groups, state in tensor memory), when at
         // least half a group holds systems, for
         //  - rows a whole plane apart (>= 64 KiB: z solves), where the rate
-        //    of row segments limits 128-byte groups: FP64 512^3 z 0.89 vs
-        //    1.18 ms, Inc 1.04 vs 1.48 ms; FP32 systems over 256 rows 0.53
-        //    vs 0.61 ms, Inc 0.63 vs 0.81 ms (shorter FP32 systems measured
-        //    faster in 128-byte groups);
-        //  - FP64 Inc solves along y (256^3: 0.151 vs 0.165 ms; 512^3 equal).
+        //    of row segments limits 128-byte groups: FP64 512^3 z 0.87 vs
+        //    1.22 ms, 256^3 0.114 vs 0.125 ms;
+        //  - FP64 Inc solves along y (256^3: 0.151 vs 0.165 ms; 512^3 equal);
+        //  - FP32 batches in the paired form (two adjacent systems a thread,
+        //    8-byte accesses; wide_pairs): z solves (512^3 0.455 vs 0.656 ms,
+        //    256^3 0.065 vs 0.071 ms), y solves of up to 256 rows (256^3
+        //    0.063 vs 0.069 ms) and Inc y solves (512^3 0.545 vs 0.578 ms).
+        //    Unpaired FP32 systems of up to 256 rows measured faster in
+        //    128-byte groups, so unpaired FP32 takes it for z solves of
+        //    over 256 rows only.
         // Along y without Inc the 128-byte form with L2 prefetch measured
-        // faster (FP64 0.857 vs 0.865 ms, FP32 0.51 vs 0.51 ms). Forced with
-        // tridForceStream(2) wherever it applies.
+        // faster otherwise (FP64 512^3 0.847 vs 0.871 ms, FP32 0.442 vs
+        // 0.454 ms). Forced with tridForceStream(2) wherever it applies.
         const int mw = wide_rows_per_thread<R>(N);
         const bool zlike = p.stride * (long long)sizeof(R) >= (1LL << 16);
-        const bool wide_auto = sizeof(R) == 8 ? (zlike || p.u != nullptr) : (zlike && N > 256);
+        bool wide_auto;
+        if (sizeof(R) == 8)
+          wide_auto = zlike || p.u != nullptr;
+        else if (wide_pairs<R>(p))
+          wide_auto = zlike || N <= 256 || p.u != nullptr;
+        else
+          wide_auto = zlike && N > 256;
         if (mw > 0 && fm == 0 && !want_tma &&
             (fs == 2 || (fs == -1 && wide_auto && 2 * p.n0 >= wide_width<R>()))) {
           plan.M = mw;
-          plan.T = 16;  // chunks per system (one warp each)
+          plan.T = wide_chunks<R>(N);  // chunks per system (one warp each)
           plan.W = wide_width<R>();
           plan.wide = true;
+          plan.pairs = wide_pairs<R>(p);
           return plan;
         }
         const int Ts = 32;

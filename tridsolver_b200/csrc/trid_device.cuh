@@ -82,6 +82,12 @@ template <typename R> __device__ __forceinline__ bool finite_rcp(R r) {
   return fabs(r) <= Limits<R>::max();
 }
 
+// The same check as one FMA per pivot, for sweeps whose per-row work is
+// issue-bound: r * 0 is a zero for a finite reciprocal and NaN for an
+// infinite or NaN one, so `acc` (starting at 0) stays finite until a pivot
+// is zero or NaN; acc != acc at the end is the verdict.
+template <typename R> __device__ __forceinline__ void pivot_acc(R &acc, R r) { acc = fma(r, R(0), acc); }
+
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 template <typename R> __device__ __forceinline__ R shfl_up(R v, int s, int w) {

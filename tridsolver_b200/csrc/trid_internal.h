@@ -22,6 +22,7 @@ struct Plan {
   bool streaming = false;           // strided: persistent streaming kernel (T = 32)
   bool wide = false;                // strided: wide streaming kernel (256-byte groups)
   bool tiles = false;               // long, contiguous: warp tiles of 512 / 1024 rows
+  bool pairs = false;               // wide, FP32: two adjacent systems per thread
   std::string describe() const;
 };
 
@@ -125,9 +126,11 @@ cudaError_t launch_strided_stream_adjoint(const BatchArgs<R> &p, const AdjointOu
 template <typename R, int M, bool INC>
 cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaStream_t st);
 // Wide streaming kernel (trid_strided_wide.cu): 256-byte groups with the
-// elimination state parked in tensor memory; rows per thread for N rows
-// (0 when it does not apply), group width, launcher.
+// elimination state parked in tensor memory; rows per thread and chunks
+// per system for N rows (0 when it does not apply), group width, launcher.
 template <typename R> int wide_rows_per_thread(int N);
+template <typename R> int wide_chunks(int N);
+template <typename R> bool wide_pairs(const BatchArgs<R> &p);
 template <typename R> int wide_width();
 template <typename R, bool INC>
 cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st);

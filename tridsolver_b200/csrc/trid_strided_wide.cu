@@ -54,26 +54,29 @@ template <typename R> constexpr int wide_w() { return 256 / (int)sizeof(R); }
 // systems per thread: 1 FP64, 2 FP32 (lanes l and l + 32 of a 64-system
 // group, two independent recurrences and the same bytes in flight)
 template <typename R> constexpr int wide_s() { return wide_w<R>() / 32; }
-// chunks per system (one warp each): 16, so 512 threads
-template <typename R> constexpr int wide_t() { return 16; }
-template <typename R> constexpr int wide_bs() { return 32 * wide_t<R>(); }
 // 32-bit TMEM columns per row: a' and c' of the thread's systems
 template <typename R> constexpr int wide_cpr() { return 2 * wide_s<R>() * (int)sizeof(R) / 4; }
 // rows per back-substitution block (one TMEM load of 32 columns; 16 for Inc)
 template <typename R, bool INC> constexpr int wide_blk() { return (INC ? 16 : 32) / wide_cpr<R>(); }
-constexpr int WIDE_SMEM_MIN = 120 * 1024;
+constexpr int WIDE_SMEM_MIN = 120 * 1024;  // one CTA per SM
+// two CTAs per SM: more than a third and at most half of the SM's 228 KiB
+// (each CTA also holds 1 KiB of the system's)
+constexpr int WIDE2_SMEM_MIN = 80 * 1024;
+constexpr int WIDE2_SMEM_MAX = 112 * 1024;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void tmem_alloc_all(uint32_t *slot) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(slot))
+// NCOL columns (a power of two, 32..512) for the CTA
+template <int NCOL> __device__ __forceinline__ void tmem_alloc_cols(uint32_t *slot) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot)),
+               "n"(NCOL)
                : "memory");
   asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
 }
-__device__ __forceinline__ void tmem_dealloc_all(uint32_t base) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(base) : "memory");
+template <int NCOL> __device__ __forceinline__ void tmem_dealloc_cols(uint32_t base) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(base), "n"(NCOL) : "memory");
 }
 __device__ __forceinline__ void tmem_fence_before_sync() {
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -180,18 +183,56 @@ __device__ __forceinline__ void wide_load_row(const BatchArgs<R> &p, const CoefP
   }
 }
 
+// The rows of two adjacent FP32 systems (PAIR: o even, pointers 8-byte
+// aligned) in one 8-byte load per array; same rules as wide_load_row.
+__device__ __forceinline__ void wide_load_pair(const BatchArgs<float> &p, long long o, bool valid, int row,
+                                               float &a0, float &a1, float &b0, float &b1, float &c0,
+                                               float &c1, float &d0, float &d1) {
+  if (valid) {
+    float2 v;
+    if (row == 0) {
+      a0 = a1 = 0.f;
+    } else {
+      v = __ldcg(reinterpret_cast<const float2 *>(p.a + o));
+      a0 = v.x;
+      a1 = v.y;
+    }
+    if (row == p.N - 1) {
+      c0 = c1 = 0.f;
+    } else {
+      v = __ldcg(reinterpret_cast<const float2 *>(p.c + o));
+      c0 = v.x;
+      c1 = v.y;
+    }
+    v = __ldcg(reinterpret_cast<const float2 *>(p.b + o));
+    b0 = v.x;
+    b1 = v.y;
+    v = __ldcg(reinterpret_cast<const float2 *>(p.d_in + o));
+    d0 = v.x;
+    d1 = v.y;
+  } else {
+    a0 = a1 = c0 = c1 = d0 = d1 = 0.f;
+    b0 = b1 = 1.f;
+  }
+}
+
 }  // namespace
 
-template <typename R, int M, int D, bool INC, typename CR = R>
-__global__ void __launch_bounds__(wide_bs<R>(), 1)
+// PAIR (FP32): thread l of a warp holds systems 2l and 2l + 1 of the group,
+// adjacent in memory, so one address and one 8-byte access serve both rows
+// (the launcher's choice when systems are contiguous along the fastest
+// dimension, whole groups, and every offset even).
+template <typename R, int M, int T, int D, bool INC, typename CR = R, int CTAS = 1, bool PAIR = false>
+__global__ void __launch_bounds__(32 * T, CTAS)
     strided_wide_kernel(const BatchArgs<R> p, const CoefPtrs<CR> coef, long long ngx, long long ngroups) {
   static_assert(std::is_same<CR, R>::value || !INC, "the promoted form has no Inc");
-  constexpr int S = wide_s<R>();  // systems per thread: lanes l and l + 32 of the group
+  static_assert(!PAIR || (sizeof(R) == 4 && std::is_same<CR, R>::value), "pairs of FP32 systems");
+  constexpr int S = wide_s<R>();  // systems per thread: lanes l and l + 32 of the group (2l, 2l + 1 PAIR)
   constexpr int W = wide_w<R>();  // = 32 * S
-  constexpr int T = wide_t<R>();
   constexpr int BS = 32 * T;
   constexpr int NWARP = BS / 32;
-  constexpr int CW = 512 / (NWARP / 4);  // TMEM columns per warp
+  constexpr int NCOL = 512 / CTAS;       // TMEM columns of the CTA
+  constexpr int CW = NCOL / (NWARP / 4);  // TMEM columns per warp
   constexpr int CPR = wide_cpr<R>();     // columns per row (a', c' of S systems)
   constexpr int B = wide_blk<R, INC>() < M ? wide_blk<R, INC>() : M;
   constexpr int NV = B * CPR;
@@ -205,7 +246,10 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
   __shared__ uint32_t tmem_slot;
   R *red = reinterpret_cast<R *>(wide_smem);
   const int tid = threadIdx.x;
-  R *sdf = red + RED + tid;  // d' of row j, system q at [(j * S + q) * BS]
+  // d' of row j, system q at [(j * S + q) * BS]; PAIR: both systems' d' as
+  // one 8-byte slot [j * BS] of sdf2
+  R *sdf = red + RED + tid;
+  float2 *sdf2 = reinterpret_cast<float2 *>(red + RED) + tid;
   const int lane = tid & 31;
   const int t = tid >> 5;    // chunk = warp
   const int warp = t;
@@ -213,7 +257,7 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
   const int row0 = t * M;
   const long long stride = p.stride;
 
-  if (warp == 0) tmem_alloc_all(&tmem_slot);
+  if (warp == 0) tmem_alloc_cols<NCOL>(&tmem_slot);
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
@@ -224,7 +268,7 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
   auto group_first = [&](long long g, int q, bool &act) -> long long {
     const long long gx = g % ngx;
     const long long i1 = g / ngx;
-    const long long i0 = gx * W + 32 * q + lane;
+    const long long i0 = gx * W + (PAIR ? 2 * lane + q : 32 * q + lane);
     act = g < ngroups && i0 < p.n0;
     return act ? i0 * p.st0 + i1 * p.st1 + (long long)row0 * stride : 0;
   };
@@ -238,17 +282,27 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
     first[q] = group_first(g, q, act[q]);
     lo[q] = first[q];
   }
+  // rows of every system of the thread into window slot k
+  auto load_rows = [&](int k, const long long (&off)[S], const bool (&act_)[S], int row) {
+    if constexpr (PAIR) {
+      wide_load_pair(p, off[0], act_[0] && row < N, row, pa[0][k], pa[1][k], pb[0][k], pb[1][k],
+                     pc[0][k], pc[1][k], pd[0][k], pd[1][k]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < S; ++q)
+        wide_load_row<R, CR>(p, coef, off[q], act_[q] && row < N, row, pa[q][k], pb[q][k], pc[q][k],
+                             pd[q][k]);
+    }
+  };
 #pragma unroll
   for (int j = 0; j < D; ++j) {
+    load_rows(j, lo, act, row0 + j);
 #pragma unroll
-    for (int q = 0; q < S; ++q) {
-      wide_load_row<R, CR>(p, coef, lo[q], act[q] && row0 + j < N, row0 + j, pa[q][j], pb[q][j],
-                           pc[q][j], pd[q][j]);
-      lo[q] += stride;
-    }
+    for (int q = 0; q < S; ++q) lo[q] += stride;
   }
 
   bool bad = false;
+  R racc = R(0);  // pivot_acc of the sweep's pivots
   for (; g < ngroups; g += gridDim.x) {
     bool actn[S];
     long long firstn[S], ln[S];
@@ -269,36 +323,42 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int k = j % D;
-      R af[S], cfr[S];
+      R af[S], cfr[S], a_[S], b_[S], c_[S], d_[S], df_[S];
 #pragma unroll
       for (int q = 0; q < S; ++q) {
-        const R a = pa[q][k], b = pb[q][k], c = pc[q][k], d = pd[q][k];
-        if (j + D < M) {
-          const int row = row0 + j + D;
-          wide_load_row<R, CR>(p, coef, lo[q], act[q] && row < N, row, pa[q][k], pb[q][k], pc[q][k],
-                               pd[q][k]);
-          lo[q] += stride;
-        } else {
-          const int row = row0 + j + D - M;
-          wide_load_row<R, CR>(p, coef, ln[q], actn[q] && row < N, row, pa[q][k], pb[q][k], pc[q][k],
-                               pd[q][k]);
-          ln[q] += stride;
-        }
+        a_[q] = pa[q][k];
+        b_[q] = pb[q][k];
+        c_[q] = pc[q][k];
+        d_[q] = pd[q][k];
+      }
+      if (j + D < M) {
+        load_rows(k, lo, act, row0 + j + D);
+#pragma unroll
+        for (int q = 0; q < S; ++q) lo[q] += stride;
+      } else {
+        load_rows(k, ln, actn, row0 + j + D - M);
+#pragma unroll
+        for (int q = 0; q < S; ++q) ln[q] += stride;
+      }
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        const R a = a_[q], b = b_[q], c = c_[q], d = d_[q];
         R df;
         if (j < 2) {
           const R r = rcp_nr(b);
-          bad |= !finite_rcp(r);
+          pivot_acc(racc, r);
           af[q] = a * r;
           cfr[q] = c * r;
           df = d * r;
         } else {
           const R r = rcp_nr(b - a * cp[q]);
-          bad |= !finite_rcp(r);
+          pivot_acc(racc, r);
           df = r * (d - a * dp[q]);
           af[q] = -r * a * ap[q];
           cfr[q] = r * c;
         }
-        sdf[(j * S + q) * BS] = df;
+        if constexpr (!PAIR) sdf[(j * S + q) * BS] = df;
+        df_[q] = df;
         if (j == 0) {
           a0[q] = af[q];
           c0[q] = cfr[q];
@@ -312,6 +372,7 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
         cp[q] = cfr[q];
         dp[q] = df;
       }
+      if constexpr (PAIR) sdf2[j * BS] = make_float2(df_[0], df_[S - 1]);
       tmem_put_row<R, S>(taddr + (uint32_t)(j * CPR), af, cfr);
     }
 
@@ -319,16 +380,29 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
     long long o[S];
     R ucur[S][INC ? B : 1], unext[S][INC ? B : 1];
 #pragma unroll
-    for (int q = 0; q < S; ++q) {
-      o[q] = first[q] + (long long)(M - 1) * stride;
+    for (int q = 0; q < S; ++q) o[q] = first[q] + (long long)(M - 1) * stride;
+    // u of rows jo - back - i (i < B) into us, o[] being at row jo
+    auto load_u = [&](R (&us)[S][INC ? B : 1], int jo, int back) {
       if constexpr (INC) {
 #pragma unroll
         for (int i = 0; i < B; ++i) {
-          const int j = M - 1 - i;
-          ucur[q][i] = (act[q] && row0 + j < N) ? __ldcg(p.u + o[q] - (long long)i * stride) : R(0);
+          const int j = jo - back - i;
+          if constexpr (PAIR) {
+            float2 v = make_float2(0.f, 0.f);
+            if (act[0] && row0 + j < N)
+              v = __ldcg(reinterpret_cast<const float2 *>(p.u + o[0] - (long long)(back + i) * stride));
+            us[0][i] = v.x;
+            us[1][i] = v.y;
+          } else {
+#pragma unroll
+            for (int q = 0; q < S; ++q)
+              us[q][i] =
+                  (act[q] && row0 + j < N) ? __ldcg(p.u + o[q] - (long long)(back + i) * stride) : R(0);
+          }
         }
       }
-    }
+    };
+    load_u(ucur, M - 1, 0);
     tmem_wait_st();
     R y[S], z[S];
 #pragma unroll
@@ -349,22 +423,25 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
     for (int bb = M / B - 1; bb >= 0; --bb) {
       uint32_t v[NV];
       tmem_get(taddr + (uint32_t)(bb * B * CPR), v);
+      // o[] is at row bb * B + B - 1 here: the next block starts B rows up
       if constexpr (INC) {
-        if (bb > 0) {
-#pragma unroll
-          for (int q = 0; q < S; ++q)
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-              const int j = bb * B - 1 - i;
-              unext[q][i] =
-                  (act[q] && row0 + j < N) ? __ldcg(p.u + o[q] - (long long)(B + i) * stride) : R(0);
-            }
-        }
+        if (bb > 0) load_u(unext, bb * B + B - 1, B);
       }
       tmem_wait_ld(v);
 #pragma unroll
       for (int i = B - 1; i >= 0; --i) {
         const int j = bb * B + i;
+        R dj[S];
+        if (j > 0 && j < M - 1) {
+          if constexpr (PAIR) {
+            const float2 dv = sdf2[j * BS];
+            dj[0] = dv.x;
+            dj[S - 1] = dv.y;
+          } else {
+#pragma unroll
+            for (int q = 0; q < S; ++q) dj[q] = sdf[(j * S + q) * BS];
+          }
+        }
 #pragma unroll
         for (int q = 0; q < S; ++q) {
           if (j < M - 1) {
@@ -373,17 +450,34 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
             } else {
               R af, cfq;
               tmem_row<R, S, NV>(v, i, q, af, cfq);
-              x[q] = sdf[(j * S + q) * BS] - af * y[q] - cfq * x[q];
+              x[q] = dj[q] - af * y[q] - cfq * x[q];
             }
           }
-          if (act[q] && row0 + j < N) {
-            if constexpr (INC)
-              p.u[o[q]] = ucur[q][B - 1 - i] + x[q];
-            else
-              p.d_out[o[q]] = x[q];
-          }
-          o[q] -= stride;
         }
+        if constexpr (PAIR) {
+          if (act[0] && row0 + j < N) {
+            float2 xv = make_float2(x[0], x[S - 1]);
+            if constexpr (INC) {
+              xv.x += ucur[0][B - 1 - i];
+              xv.y += ucur[S - 1][B - 1 - i];
+              *reinterpret_cast<float2 *>(p.u + o[0]) = xv;
+            } else {
+              *reinterpret_cast<float2 *>(p.d_out + o[0]) = xv;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < S; ++q) {
+            if (act[q] && row0 + j < N) {
+              if constexpr (INC)
+                p.u[o[q]] = ucur[q][B - 1 - i] + x[q];
+              else
+                p.d_out[o[q]] = x[q];
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < S; ++q) o[q] -= stride;
       }
       if constexpr (INC) {
 #pragma unroll
@@ -399,36 +493,56 @@ __global__ void __launch_bounds__(wide_bs<R>(), 1)
       lo[q] = ln[q];
     }
   }
+  bad |= racc != racc;
   report_bad_pivot(bad, p.flag);
 
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
-  if (warp == 0) tmem_dealloc_all(tbase);
+  if (warp == 0) tmem_dealloc_cols<NCOL>(tbase);
 }
 
 template <typename R> int wide_width() { return wide_w<R>(); }
 
-// Rows per thread for a system of N rows (64 < N <= 512), 0 if none.
-template <typename R> int wide_rows_per_thread(int N) {
-  constexpr int T = wide_t<R>();
-  if (N <= 64 || N > 512) return 0;
-  if (N <= 8 * T) return 8;
-  if (N <= 16 * T) return 16;
-  return N <= 32 * T ? 32 : 0;
+// FP32 batches that take the paired form: systems contiguous along the
+// fastest dimension, whole groups, even offsets and 8-byte aligned arrays.
+template <typename R> bool wide_pairs(const BatchArgs<R> &p) {
+  if (sizeof(R) != 4) return false;
+  auto al8 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 7u) == 0; };
+  return p.st0 == 1 && p.n0 % wide_w<R>() == 0 && p.st1 % 2 == 0 && p.stride % 2 == 0 && al8(p.a) &&
+         al8(p.b) && al8(p.c) && al8(p.d_in) && al8(p.d_out) && (!p.u || al8(p.u));
 }
 
-template <typename R, int M, bool INC, typename CR = R>
+// Chunks (warps) per system and rows per chunk for a system of N rows
+// (64 < N <= 512; 0 if none). Systems of up to 256 rows: 8 chunks of up to
+// 32 rows, 256-thread CTAs with 256 TMEM columns each, two per SM, so one
+// CTA's reduced solve and back-substitution overlap the other's streaming
+// (FP32 256^3 z: 0.072 -> X ms); longer ones: 16 chunks of 32 rows, one
+// 512-thread CTA with all 512 columns per SM.
+template <typename R> int wide_chunks(int N) { return N <= 64 || N > 512 ? 0 : N <= 256 ? 8 : 16; }
+template <typename R> int wide_rows_per_thread(int N) {
+  if (N <= 64 || N > 512) return 0;
+  return N <= 128 ? 16 : 32;
+}
+
+template <typename R, int M, int T, bool INC, typename CR = R>
 static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
                                  const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
   constexpr int W = wide_w<R>();
-  constexpr int T = wide_t<R>();
   constexpr int BS = 32 * T;
+  constexpr int CTAS = T == 8 ? 2 : 1;
   constexpr int D = 4;
   const size_t red = ((size_t)6 * T * 33 * sizeof(R) + 15) / 16 * 16;
   size_t smem = red + (size_t)M * wide_s<R>() * BS * sizeof(R);
-  if (smem < (size_t)WIDE_SMEM_MIN) smem = WIDE_SMEM_MIN;  // one CTA per SM
-  auto kern = strided_wide_kernel<R, M, D, INC, CR>;
+  // the shared-memory request caps the CTAs per SM at CTAS, so every CTA's
+  // TMEM allocation is granted without waiting
+  const size_t smem_min = CTAS == 2 ? WIDE2_SMEM_MIN : WIDE_SMEM_MIN;
+  if (smem < smem_min) smem = smem_min;
+  if (CTAS == 2 && smem > WIDE2_SMEM_MAX) return cudaErrorInvalidValue;
+  auto kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS>;
+  if constexpr (sizeof(R) == 4 && std::is_same<CR, R>::value) {
+    if (wide_pairs<R>(p)) kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS, true>;
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long ngx = (p.n0 + W - 1) / W;
@@ -436,31 +550,31 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long grid = ngroups < sms ? ngroups : sms;
+  const long long cap = (long long)sms * CTAS;
+  const long long grid = ngroups < cap ? ngroups : cap;
   kern<<<(unsigned)grid, BS, smem, st>>>(p, cf, ngx, ngroups);
   return cudaGetLastError();
 }
 
+template <typename R, bool INC, typename CR = R>
+static cudaError_t launch_wide_n(const BatchArgs<R> &p, cudaStream_t st,
+                                 const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
+  if (p.N <= 64 || p.N > 512) return cudaErrorInvalidValue;
+  if (p.N <= 128) return launch_wide_m<R, 16, 8, INC, CR>(p, st, cf);
+  if (p.N <= 256) return launch_wide_m<R, 32, 8, INC, CR>(p, st, cf);
+  return launch_wide_m<R, 32, 16, INC, CR>(p, st, cf);
+}
+
 template <typename R, bool INC>
 cudaError_t launch_strided_wide(const BatchArgs<R> &p, cudaStream_t st) {
-  switch (wide_rows_per_thread<R>(p.N)) {
-    case 8: return launch_wide_m<R, 8, INC>(p, st);
-    case 16: return launch_wide_m<R, 16, INC>(p, st);
-    case 32: return launch_wide_m<R, 32, INC>(p, st);
-    default: return cudaErrorInvalidValue;
-  }
+  return launch_wide_n<R, INC>(p, st);
 }
 
 // Promoted solve: FP64 arithmetic on FP32-stored coefficients (cf), p.a,
 // p.b, p.c unused; 64 < N <= 512.
 cudaError_t launch_strided_wide_promoted(const BatchArgs<double> &p, const CoefPtrs<float> &cf,
                                          cudaStream_t st) {
-  switch (wide_rows_per_thread<double>(p.N)) {
-    case 8: return launch_wide_m<double, 8, false, float>(p, st, cf);
-    case 16: return launch_wide_m<double, 16, false, float>(p, st, cf);
-    case 32: return launch_wide_m<double, 32, false, float>(p, st, cf);
-    default: return cudaErrorInvalidValue;
-  }
+  return launch_wide_n<double, false, float>(p, st, cf);
 }
 
 template cudaError_t launch_strided_wide<double, false>(const BatchArgs<double> &, cudaStream_t);
@@ -471,5 +585,9 @@ template int wide_width<double>();
 template int wide_width<float>();
 template int wide_rows_per_thread<double>(int);
 template int wide_rows_per_thread<float>(int);
+template int wide_chunks<double>(int);
+template bool wide_pairs<double>(const BatchArgs<double> &);
+template bool wide_pairs<float>(const BatchArgs<float> &);
+template int wide_chunks<float>(int);
 
 }  // namespace trid
