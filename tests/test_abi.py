@@ -168,9 +168,9 @@ def test_release_scratch_reports_missing_device():
     (8, [7, 512, 3], 1, "hybrid M=8 T=64 W=8"),
     (8, [8, 512, 3], 1, "hybrid M=16 T=32 W=16 stream"),
     (4, [512, 512, 512], 2, "hybrid M=32 T=16 W=64 wide pairs"),
-    (4, [256, 256, 256], 2, "hybrid M=32 T=8 W=64 wide pairs"),
+    (4, [256, 256, 256], 2, "hybrid M=16 T=16 W=64 wide pairs"),
     (4, [512, 512, 512], 1, "hybrid M=16 T=32 W=32 stream"),
-    (4, [256, 256, 256], 1, "hybrid M=32 T=8 W=64 wide pairs"),
+    (4, [256, 256, 256], 1, "hybrid M=16 T=16 W=64 wide pairs"),
     (4, [128, 100, 2], 1, "hybrid M=16 T=8 W=64 wide pairs"),
     (4, [96, 100, 2], 1, "hybrid M=8 T=16 W=32 stream"),
     (4, [96, 200, 2], 1, "hybrid M=16 T=16 W=32 stream"),

@@ -143,22 +143,23 @@ Plan choose_plan_forced(const BatchArgs<R> &p, bool aligned16, const Forces &f) 
         // Along y without Inc the 128-byte form with L2 prefetch measured
         // faster otherwise (FP64 512^3 0.847 vs 0.871 ms, FP32 0.442 vs
         // 0.454 ms). Forced with tridForceStream(2) wherever it applies.
-        const int mw = wide_rows_per_thread<R>(N);
+        const bool pairs = wide_pairs<R>(p);
+        const int mw = wide_rows_per_thread<R>(N, pairs);
         const bool zlike = p.stride * (long long)sizeof(R) >= (1LL << 16);
         bool wide_auto;
         if (sizeof(R) == 8)
           wide_auto = zlike || p.u != nullptr;
-        else if (wide_pairs<R>(p))
+        else if (pairs)
           wide_auto = zlike || N <= 256 || p.u != nullptr;
         else
           wide_auto = zlike && N > 256;
         if (mw > 0 && fm == 0 && !want_tma &&
             (fs == 2 || (fs == -1 && wide_auto && 2 * p.n0 >= wide_width<R>()))) {
           plan.M = mw;
-          plan.T = wide_chunks<R>(N);  // chunks per system (one warp each)
+          plan.T = wide_chunks<R>(N, pairs);  // chunks per system (one warp each)
           plan.W = wide_width<R>();
           plan.wide = true;
-          plan.pairs = wide_pairs<R>(p);
+          plan.pairs = pairs;
           return plan;
         }
         const int Ts = 32;

@@ -128,8 +128,8 @@ cudaError_t launch_strided_stream(const BatchArgs<R> &p, const Plan &plan, cudaS
 // Wide streaming kernel (trid_strided_wide.cu): 256-byte groups with the
 // elimination state parked in tensor memory; rows per thread and chunks
 // per system for N rows (0 when it does not apply), group width, launcher.
-template <typename R> int wide_rows_per_thread(int N);
-template <typename R> int wide_chunks(int N);
+template <typename R> int wide_rows_per_thread(int N, bool pairs);
+template <typename R> int wide_chunks(int N, bool pairs);
 template <typename R> bool wide_pairs(const BatchArgs<R> &p);
 template <typename R> int wide_width();
 template <typename R, bool INC>

@@ -20,17 +20,22 @@
 //   - the chunk's top reduced row is accumulated in forward order during the
 //     forward sweep (x_1 = P + Q x_0 + S x_{k+1} as rows k are eliminated), so
 //     the parked state is read back once, by the back-substitution.
-// The CTA (512 threads: 16 warps, warp t = chunk t of every system of the
-// group; lane l holds system l, and in FP32 also system l + 32, so a 64-
-// system FP32 group keeps the same bytes in flight as a 32-system FP64 one,
-// with two independent recurrences per thread) is persistent and walks over
-// groups; each thread streams its chunk's rows through a D-deep register
-// window that runs on into the next group, so loads stay in flight across
-// the reduced solve and the stores. The reduced systems are solved 32 at a
-// time (once per system of a thread).
-// The dynamic shared memory request is at least 120 KiB, so one CTA runs per
-// SM and the 512-column allocation never waits for another CTA of this
-// kernel. Every path through the kernel reaches the deallocation at its end.
+// A CTA (T warps, warp t = chunk t of every system of the group; lane l
+// holds system l, and in FP32 a second system: l + 32, or in the paired form
+// the adjacent systems 2l and 2l + 1, which share one address and one 8-byte
+// access per array; so a 64-system FP32 group keeps the same bytes in flight
+// as a 32-system FP64 one, with two independent recurrences per thread) is
+// persistent and walks over groups; each thread streams its chunk's rows
+// through a D-deep register window that runs on into the next group, so
+// loads stay in flight across the reduced solve and the stores. The reduced
+// systems are solved 32 at a time (once per system of a thread).
+// A CTA of 16 chunks (512 threads) takes all 512 TMEM columns and runs alone
+// on its SM (a dynamic shared memory request of at least 120 KiB); a CTA of
+// 8 chunks (256 threads) takes 256 columns and runs two per SM (80-112 KiB
+// each), so one CTA's reduced solve and back-substitution overlap the
+// other's streaming. Either way the shared-memory request caps the CTAs per
+// SM, so an allocation never waits for another CTA of this kernel. Every
+// path through the kernel reaches the deallocation at its end.
 //
 // Inc variants load u block by block during the back-substitution (one
 // block ahead, the first block before the reduced solve).
@@ -51,8 +56,9 @@ namespace trid {
 namespace {
 
 template <typename R> constexpr int wide_w() { return 256 / (int)sizeof(R); }
-// systems per thread: 1 FP64, 2 FP32 (lanes l and l + 32 of a 64-system
-// group, two independent recurrences and the same bytes in flight)
+// systems per thread: 1 FP64, 2 FP32 (systems l and l + 32 of a 64-system
+// group, or 2l and 2l + 1 in the paired form: two independent recurrences
+// and the same bytes in flight)
 template <typename R> constexpr int wide_s() { return wide_w<R>() / 32; }
 // 32-bit TMEM columns per row: a' and c' of the thread's systems
 template <typename R> constexpr int wide_cpr() { return 2 * wide_s<R>() * (int)sizeof(R) / 4; }
@@ -234,7 +240,9 @@ __global__ void __launch_bounds__(32 * T, CTAS)
   constexpr int NCOL = 512 / CTAS;       // TMEM columns of the CTA
   constexpr int CW = NCOL / (NWARP / 4);  // TMEM columns per warp
   constexpr int CPR = wide_cpr<R>();     // columns per row (a', c' of S systems)
-  constexpr int B = wide_blk<R, INC>() < M ? wide_blk<R, INC>() : M;
+  // back-substitution blocks of 16 columns under a deep window
+  constexpr int BK = D >= 8 ? 16 / CPR : wide_blk<R, INC>();
+  constexpr int B = BK < M ? BK : M;
   constexpr int NV = B * CPR;
   static_assert(NV == 16 || NV == 32, "one TMEM load per block");
   static_assert(NWARP % 4 == 0, "whole lane quarters");
@@ -514,15 +522,25 @@ template <typename R> bool wide_pairs(const BatchArgs<R> &p) {
 }
 
 // Chunks (warps) per system and rows per chunk for a system of N rows
-// (64 < N <= 512; 0 if none). Systems of up to 256 rows: 8 chunks of up to
-// 32 rows, 256-thread CTAs with 256 TMEM columns each, two per SM, so one
-// CTA's reduced solve and back-substitution overlap the other's streaming
-// (FP32 256^3 z: 0.072 -> X ms); longer ones: 16 chunks of 32 rows, one
-// 512-thread CTA with all 512 columns per SM.
-template <typename R> int wide_chunks(int N) { return N <= 64 || N > 512 ? 0 : N <= 256 ? 8 : 16; }
-template <typename R> int wide_rows_per_thread(int N) {
+// (64 < N <= 512; 0 if none), `pairs` when the batch takes the paired form.
+//   - Systems of up to 256 rows: 8 chunks of up to 32 rows, 256-thread CTAs
+//     with 256 TMEM columns each, two per SM (FP64 256^3 z: 0.129 -> 0.114
+//     ms against 16 chunks of 16 rows at one CTA per SM);
+//   - paired FP32 systems of 129-256 rows: 16 chunks of 16 rows, one CTA
+//     per SM with an 8-row window (fraction of the copy bandwidth at 256^3,
+//     y / y Inc / z / z Inc: 0.83 / 0.85 / 0.82 / 0.83, against 0.81 / 0.81
+//     / 0.79 / 0.78 with two CTAs of 8 chunks: 1024 groups fill 6.9 rounds
+//     of 148 CTAs but only 3.5 of 296, and the deeper window pays for the
+//     reduced solve that no second CTA overlaps);
+//   - longer systems: 16 chunks of 32 rows, one 512-thread CTA per SM.
+template <typename R> int wide_chunks(int N, bool pairs) {
   if (N <= 64 || N > 512) return 0;
-  return N <= 128 ? 16 : 32;
+  return N > 256 || (pairs && N > 128) ? 16 : 8;
+}
+template <typename R> int wide_rows_per_thread(int N, bool pairs) {
+  if (N <= 64 || N > 512) return 0;
+  if (N <= 128) return 16;
+  return N <= 256 && pairs ? 16 : 32;
 }
 
 template <typename R, int M, int T, bool INC, typename CR = R>
@@ -531,7 +549,8 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
   constexpr int W = wide_w<R>();
   constexpr int BS = 32 * T;
   constexpr int CTAS = T == 8 ? 2 : 1;
-  constexpr int D = 4;
+  // (the 8-row window is for the paired FP32 form; unpaired it spills)
+  constexpr int D = (sizeof(R) == 4 && T == 16 && M == 16) ? 8 : 4;
   const size_t red = ((size_t)6 * T * 33 * sizeof(R) + 15) / 16 * 16;
   size_t smem = red + (size_t)M * wide_s<R>() * BS * sizeof(R);
   // the shared-memory request caps the CTAs per SM at CTAS, so every CTA's
@@ -539,9 +558,16 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
   const size_t smem_min = CTAS == 2 ? WIDE2_SMEM_MIN : WIDE_SMEM_MIN;
   if (smem < smem_min) smem = smem_min;
   if (CTAS == 2 && smem > WIDE2_SMEM_MAX) return cudaErrorInvalidValue;
-  auto kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS>;
-  if constexpr (sizeof(R) == 4 && std::is_same<CR, R>::value) {
-    if (wide_pairs<R>(p)) kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS, true>;
+  void (*kern)(const BatchArgs<R>, const CoefPtrs<CR>, long long, long long) = nullptr;
+  if constexpr (D == 8) {
+    // (wide_chunks gives this shape to the paired form only)
+    if (!wide_pairs<R>(p)) return cudaErrorInvalidValue;
+    kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS, true>;
+  } else {
+    kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS>;
+    if constexpr (sizeof(R) == 4 && std::is_same<CR, R>::value) {
+      if (wide_pairs<R>(p)) kern = strided_wide_kernel<R, M, T, D, INC, CR, CTAS, true>;
+    }
   }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -559,10 +585,16 @@ static cudaError_t launch_wide_m(const BatchArgs<R> &p, cudaStream_t st,
 template <typename R, bool INC, typename CR = R>
 static cudaError_t launch_wide_n(const BatchArgs<R> &p, cudaStream_t st,
                                  const CoefPtrs<CR> &cf = CoefPtrs<CR>{}) {
-  if (p.N <= 64 || p.N > 512) return cudaErrorInvalidValue;
-  if (p.N <= 128) return launch_wide_m<R, 16, 8, INC, CR>(p, st, cf);
-  if (p.N <= 256) return launch_wide_m<R, 32, 8, INC, CR>(p, st, cf);
-  return launch_wide_m<R, 32, 16, INC, CR>(p, st, cf);
+  bool pairs = false;
+  if constexpr (std::is_same<CR, R>::value) pairs = wide_pairs<R>(p);
+  const int T = wide_chunks<R>(p.N, pairs), M = wide_rows_per_thread<R>(p.N, pairs);
+  if (T == 8 && M == 16) return launch_wide_m<R, 16, 8, INC, CR>(p, st, cf);
+  if (T == 8 && M == 32) return launch_wide_m<R, 32, 8, INC, CR>(p, st, cf);
+  if (T == 16 && M == 32) return launch_wide_m<R, 32, 16, INC, CR>(p, st, cf);
+  if constexpr (sizeof(R) == 4 && std::is_same<CR, R>::value) {
+    if (T == 16 && M == 16) return launch_wide_m<R, 16, 16, INC, CR>(p, st, cf);
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <typename R, bool INC>
@@ -583,11 +615,11 @@ template cudaError_t launch_strided_wide<float, false>(const BatchArgs<float> &,
 template cudaError_t launch_strided_wide<float, true>(const BatchArgs<float> &, cudaStream_t);
 template int wide_width<double>();
 template int wide_width<float>();
-template int wide_rows_per_thread<double>(int);
-template int wide_rows_per_thread<float>(int);
-template int wide_chunks<double>(int);
+template int wide_rows_per_thread<double>(int, bool);
+template int wide_rows_per_thread<float>(int, bool);
+template int wide_chunks<double>(int, bool);
 template bool wide_pairs<double>(const BatchArgs<double> &);
 template bool wide_pairs<float>(const BatchArgs<float> &);
-template int wide_chunks<float>(int);
+template int wide_chunks<float>(int, bool);
 
 }  // namespace trid
