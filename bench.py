@@ -477,7 +477,7 @@ def config_sweep(dev, hbm):
                     out.append({"grid": n, "dtype": name, "axis": "xyz"[axis], "inc": inc,
                                 "ms": round(ms, 4), "elements_per_s": n ** 3 / ms * 1e3,
                                 "hbm_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
-                                "plan": tb.describe_plan(es, dims, axis)})
+                                "plan": tb.describe_plan(es, dims, axis, inc=inc)})
             del a, b, c, d, u
             torch.cuda.empty_cache()
     return out

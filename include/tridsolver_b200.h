@@ -367,4 +367,10 @@ EXTERN_C tridStatus_t tridDmtsvStridedBatchNoAlloc(const TridParams *ctx, const 
 EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
                               const int *pads, char *buf, int buflen);
 
+/* As tridDescribePlan, for the Inc variant of the solve when inc != 0 (its
+ * plan may differ: u is a fifth stream of every row). Arrays are taken as
+ * aligned. Returns the length. */
+EXTERN_C int tridDescribePlanInc(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                                 const int *pads, int inc, char *buf, int buflen);
+
 #endif

@@ -191,6 +191,18 @@ def test_plan_table(dtype_bytes, dims, solvedim, expect):
     assert tb.describe_plan(dtype_bytes, dims, solvedim).startswith(expect)
 
 
+@pytest.mark.parametrize("dtype_bytes,dims,solvedim,expect", [
+    (4, [512, 512, 512], 1, "hybrid M=32 T=16 W=64 wide pairs"),
+    (8, [512, 512, 512], 1, "hybrid M=32 T=16 W=32 wide"),
+    (8, [512, 512, 512], 2, "hybrid M=32 T=16 W=32 wide"),
+    (4, [96, 200, 2], 1, "hybrid M=8 T=32 W=32 stream"),
+])
+def test_plan_table_inc(dtype_bytes, dims, solvedim, expect):
+    """The Inc variant's plan (u a fifth stream): the wide kernel takes FP64
+    and paired FP32 Inc solves along y too."""
+    assert tb.describe_plan(dtype_bytes, dims, solvedim, inc=True).startswith(expect)
+
+
 def test_force_plan_round_trip():
     tb.force_plan(tb.FAMILY_PCR)
     assert tb.describe_plan(8, [20, 10], 0).startswith("pcr M=1 T=32")

@@ -41,6 +41,7 @@ SYMBOLS = {
     "tridForceTma": (_I, [_I]),
     "tridForceStream": (_I, [_I]),
     "tridDescribePlan": (_I, [_I, _I, _I, _IP, _IP, ctypes.c_char_p, _I]),
+    "tridDescribePlanInc": (_I, [_I, _I, _I, _IP, _IP, _I, ctypes.c_char_p, _I]),
     "tridDmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
     "tridSmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
     "tridRaggedAutotune": (_I, [_I]),

@@ -282,11 +282,11 @@ def set_mixed_mode(mode=0):
         raise TridError(st, "tridSetMixedMode")
 
 
-def describe_plan(dtype_bytes, dims, solvedim, pads=None):
+def describe_plan(dtype_bytes, dims, solvedim, pads=None, inc=False):
     pads = dims if pads is None else pads
     buf = ctypes.create_string_buffer(128)
-    n = _lib.load().tridDescribePlan(int(dtype_bytes), len(dims), int(solvedim), _ints(dims),
-                                     _ints(pads), buf, 128)
+    n = _lib.load().tridDescribePlanInc(int(dtype_bytes), len(dims), int(solvedim), _ints(dims),
+                                        _ints(pads), int(bool(inc)), buf, 128)
     if n < 0:
         raise TridError(TridStatus.INVALID_VALUE, "tridDescribePlan")
     return buf.value.decode()

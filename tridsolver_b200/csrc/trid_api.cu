@@ -426,23 +426,23 @@ EXTERN_C tridStatus_t tridSetMixedMode(int mode) {
   return TRID_STATUS_SUCCESS;
 }
 
-EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
-                              const int *pads, char *buf, int buflen) {
+EXTERN_C int tridDescribePlanInc(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                                 const int *pads, int inc, char *buf, int buflen) {
   std::string desc;
   bool empty = false;
   // alignment is taken as satisfied: the description is of the shape only
   if (dtype_bytes == 8) {
     BatchArgs<double> p;
     double *dummy = reinterpret_cast<double *>(256);
-    if (make_batch<double>(dummy, dummy, dummy, dummy, nullptr, false, ndim, solvedim, dims, pads,
-                           &p, &empty) != TRID_STATUS_SUCCESS)
+    if (make_batch<double>(dummy, dummy, dummy, dummy, inc ? dummy : nullptr, inc != 0, ndim, solvedim,
+                           dims, pads, &p, &empty) != TRID_STATUS_SUCCESS)
       return -1;
     desc = empty ? "empty" : choose_plan<double>(p, vec_aligned<double>(p)).describe();
   } else if (dtype_bytes == 4) {
     BatchArgs<float> p;
     float *dummy = reinterpret_cast<float *>(256);
-    if (make_batch<float>(dummy, dummy, dummy, dummy, nullptr, false, ndim, solvedim, dims, pads, &p,
-                          &empty) != TRID_STATUS_SUCCESS)
+    if (make_batch<float>(dummy, dummy, dummy, dummy, inc ? dummy : nullptr, inc != 0, ndim, solvedim,
+                          dims, pads, &p, &empty) != TRID_STATUS_SUCCESS)
       return -1;
     desc = empty ? "empty" : choose_plan<float>(p, vec_aligned<float>(p)).describe();
   } else {
@@ -453,4 +453,9 @@ EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int
     buf[buflen - 1] = '\0';
   }
   return (int)desc.size();
+}
+
+EXTERN_C int tridDescribePlan(int dtype_bytes, int ndim, int solvedim, const int *dims,
+                              const int *pads, char *buf, int buflen) {
+  return tridDescribePlanInc(dtype_bytes, ndim, solvedim, dims, pads, 0, buf, buflen);
 }
