@@ -22,11 +22,17 @@
 // a second-level tridiagonal system (2 rows per tile, at most 64 rows), and
 // the warp that finishes the last tile of a system solves it with one warp
 // PCR and publishes every tile's first and last unknown. The other warps of
-// the system wait for that (a bounded wait on a flag) while keeping their
-// tile in registers, then substitute and store. So every element is read
-// once and written once, with 8 values of scratch per tile. Claims are in
-// system order, so the tiles a warp waits for are held by running warps:
-// the wait always ends.
+// the system park their tile's eliminated rows in tensor memory (96 32-bit
+// columns of the warp's lane quarter), take their next item, and only after
+// publishing that one (or after a warp item) wait (bounded, on a flag) for
+// the parked tile's system, then substitute and store. So every element is
+// read once and written once, with 8 values of scratch per tile, and a wait
+// has a whole item of slack (the earlier form held the tile in registers and
+// waited at once: 17 us a wait on average, a third of the warps' time).
+// A warp holds at most one parked tile, in one of its two TMEM slots; each
+// claimed tile is published before its warp waits on anything, and claims
+// are in system order, so the tiles a warp waits for are held by running
+// warps: the wait always ends.
 //
 // The reference has no ragged entry point; its per-system solve trid_scalar
 // (scalar/src/cpu/trid_cpu.cpp:312-353) is the oracle for each system.
@@ -38,6 +44,7 @@
 
 #include "trid_internal.h"
 #include "trid_tile.cuh"
+#include "trid_tmem.cuh"
 #include "tridsolver_b200.h"
 
 namespace trid {
@@ -191,9 +198,61 @@ __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base
   }
 }
 
+
+// TMEM per CTA: one parking slot in each warp's lane quarter, 96 columns
+// (a', c', d' of the lane's interior rows 1 .. M-2 and the reduced solve's
+// y[3], z[3], as 32-bit words) of the CTA's 128.
+constexpr int kRaggedTmemCols = 128;
+
+template <typename R> constexpr int park_words() { return (sizeof(R) / 4) * (3 * (tile_m<R>() - 2) + 6); }
+static_assert(park_words<double>() == 96 && park_words<float>() == 96, "three 32-column transfers");
+
+// The values of a parked tile, one 32-bit word array per 32 columns.
+template <typename R> struct ParkWords {
+  uint32_t w[3][32];
+  __device__ __forceinline__ void put(int k, R v) {
+    if constexpr (sizeof(R) == 8) {
+      w[(2 * k) / 32][(2 * k) % 32] = (uint32_t)__double2loint(v);
+      w[(2 * k + 1) / 32][(2 * k + 1) % 32] = (uint32_t)__double2hiint(v);
+    } else {
+      w[k / 32][k % 32] = __float_as_uint(v);
+    }
+  }
+  __device__ __forceinline__ R get(int k) const {
+    if constexpr (sizeof(R) == 8)
+      return __hiloint2double((int)w[(2 * k + 1) / 32][(2 * k + 1) % 32], (int)w[(2 * k) / 32][(2 * k) % 32]);
+    else
+      return __uint_as_float(w[k / 32][k % 32]);
+  }
+};
+
+// x of the tile from its rows after elimination (a, c, d: rows 0 .. M-1,
+// rows 1 .. M-2 interior) and the tile's first and last unknowns, out through
+// the warp's d rows with coalesced element stores.
 template <typename R>
-__device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item, R *buf, int lane,
-                                          bool &bad) {
+__device__ __forceinline__ void tile_store(const RaggedArgs<R> &p, long long base, int nt,
+                                           R (&a)[tile_m<R>()], R (&c)[tile_m<R>()],
+                                           R (&d)[tile_m<R>()], R yy, R zz, R *buf, int lane) {
+  using L = SmemLayout<R, tile_m<R>()>;
+  chunk_substitute<R, tile_m<R>()>(a, c, d, yy, zz);
+  sts_row<R, tile_m<R>()>(buf + 3 * L::BUF + lane * L::ROW, d);
+  __syncwarp();
+#pragma unroll 4
+  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
+  __syncwarp();  // the buffer is free for the next item
+}
+
+// Tile item, first part: stage, eliminate, reduce, publish the tile's two
+// second-level rows. A system of one tile, or the warp whose tile completes
+// its system (which then solves the second level and publishes its
+// solution), finishes the tile at once (false). Otherwise the tile's state
+// is left in `pw` for parking (true): the warp
+// finishes it after its next item's first part, so the wait for the rest of
+// the system overlaps useful work. No wait happens here, so every claimed
+// tile is published without depending on any other.
+template <typename R>
+__device__ __forceinline__ bool tile_publish(const RaggedArgs<R> &p, long long item, R *buf, int lane,
+                                             ParkWords<R> &pw, bool &bad) {
   using L = SmemLayout<R, tile_m<R>()>;
   const int4 meta = p.tile_meta[item];
   const int s = meta.x;
@@ -207,9 +266,8 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
   stage_tile_rows<R>(p.a, p.b, p.c, p.d, p.vec16, base0 + r0, nt, buf, lane);
 
   constexpr int kTM = tile_m<R>();
-  R a[kTM], b[kTM], c[kTM], d[kTM];
+  R a[kTM], c[kTM], d[kTM];
   lds_row<R, kTM>(buf + 0 * L::BUF + lane * L::ROW, a);
-  lds_row<R, kTM>(buf + 1 * L::BUF + lane * L::ROW, b);
   lds_row<R, kTM>(buf + 2 * L::BUF + lane * L::ROW, c);
   lds_row<R, kTM>(buf + 3 * L::BUF + lane * L::ROW, d);
   const long long row0 = r0 + (long long)lane * kTM;
@@ -217,92 +275,203 @@ __device__ __forceinline__ void tile_item(const RaggedArgs<R> &p, long long item
 #pragma unroll
   for (int i = 0; i < kTM; ++i)
     if (row0 + i == n - 1) c[i] = R(0);
-  chunk_forward<R, kTM, true>(a, b, c, d, bad);
+  chunk_forward_staged<R, kTM>(a, buf + 1 * L::BUF + lane * L::ROW, c, d, bad);
   chunk_backward<R, kTM, true>(a, c, d, bad);
   const Row<R> top{a[0], c[0], d[0]}, bot{a[kTM - 1], c[kTM - 1], d[kTM - 1]};
   R y[3], z[3];
   reduced_solve3<R>(top, bot, lane == 0 ? -top.A : R(0), lane == 31 ? -bot.C : R(0), lane, y, z,
                     bad);
-  R yy = y[0], zz = z[0];
-  if (K > 1) {
-    // the tile's first unknown f = y(lane 0) and last l = z(lane 31), each
-    // as p + alpha x_prev + beta x_next
-    const R pf = shfl_idx(y[0], 0, 32), af = shfl_idx(y[1], 0, 32), bf = shfl_idx(y[2], 0, 32);
-    const R pl = shfl_idx(z[0], 31, 32), al = shfl_idx(z[1], 31, 32), bl = shfl_idx(z[2], 31, 32);
-    bool last = false;
-    if (lane == 0) {
-      Row<R> t2, b2;
-      second_level_rows<R>(pf, af, bf, pl, al, bl, j == 0, j == K - 1, t2, b2);
-      R *tr = p.tile_rows + 6 * (ts + j);
-      tr[0] = t2.A;
-      tr[1] = t2.C;
-      tr[2] = t2.D;
-      tr[3] = b2.A;
-      tr[4] = b2.C;
-      tr[5] = b2.D;
-      // release: the rows before the count; acquire: the other tiles' rows
-      // for the warp that completes the count
-      last = atomic_add_acq_rel(&p.sys_done[s], 1u) == (unsigned)(K - 1);
+  if (K == 1) {
+    tile_store<R>(p, base0 + r0, nt, a, c, d, y[0], z[0], buf, lane);
+    return false;
+  }
+  // the tile's first unknown f = y(lane 0) and last l = z(lane 31), each
+  // as p + alpha x_prev + beta x_next
+  const R pf = shfl_idx(y[0], 0, 32), af = shfl_idx(y[1], 0, 32), bf = shfl_idx(y[2], 0, 32);
+  const R pl = shfl_idx(z[0], 31, 32), al = shfl_idx(z[1], 31, 32), bl = shfl_idx(z[2], 31, 32);
+  bool last = false;
+  if (lane == 0) {
+    Row<R> t2, b2;
+    second_level_rows<R>(pf, af, bf, pl, al, bl, j == 0, j == K - 1, t2, b2);
+    R *tr = p.tile_rows + 6 * (ts + j);
+    tr[0] = t2.A;
+    tr[1] = t2.C;
+    tr[2] = t2.D;
+    tr[3] = b2.A;
+    tr[4] = b2.C;
+    tr[5] = b2.D;
+    // release: the rows before the count; acquire: the other tiles' rows
+    // for the warp that completes the count
+    last = atomic_add_acq_rel(&p.sys_done[s], 1u) == (unsigned)(K - 1);
+  }
+  last = __shfl_sync(FULL_MASK, last, 0);
+  if (last) {
+    __syncwarp();
+    Row<R> t2{R(0), R(0), R(0)}, b2{R(0), R(0), R(0)};
+    if (lane < K) {
+      const R *tr = p.tile_rows + 6 * (ts + lane);  // read from L2, not a stale L1 line
+      t2 = Row<R>{__ldcg(tr + 0), __ldcg(tr + 1), __ldcg(tr + 2)};
+      b2 = Row<R>{__ldcg(tr + 3), __ldcg(tr + 4), __ldcg(tr + 5)};
     }
-    last = __shfl_sync(FULL_MASK, last, 0);
-    if (last) {
-      __syncwarp();
-      Row<R> t2{R(0), R(0), R(0)}, b2{R(0), R(0), R(0)};
-      if (lane < K) {
-        const R *tr = p.tile_rows + 6 * (ts + lane);  // read from L2, not a stale L1 line
-        t2 = Row<R>{__ldcg(tr + 0), __ldcg(tr + 1), __ldcg(tr + 2)};
-        b2 = Row<R>{__ldcg(tr + 3), __ldcg(tr + 4), __ldcg(tr + 5)};
-      }
-      R f, l;
-      reduced_solve<R>(t2, b2, lane, 32, f, l, bad);
-      if (lane < K) {
-        p.tile_fl[2 * (ts + lane)] = f;
-        p.tile_fl[2 * (ts + lane) + 1] = l;
-      }
-      __threadfence();
-      __syncwarp();
-      if (lane == 0 && !p.withhold) atomicExch(&p.sys_ready[s], 1u);
-    } else {
-      unsigned ok = 1;
-      if (lane == 0) {
-        // bounded: p.wait_limit polls (kWaitLimit unless a test lowered
-        // it), and none at all once any wait of this launch has given up
-        // (error != 0)
-        const volatile unsigned *err = p.error;
-        unsigned it = 0;
-        unsigned r = load_acquire(p.sys_ready + s);
-        while (r == 0u && *err == 0u && it < p.wait_limit) {
-          __nanosleep(128);
-          ++it;
-          r = load_acquire(p.sys_ready + s);
-        }
-        ok = r != 0u;
-        if (!ok) atomicExch(p.error, 2u);
-      }
-      ok = __shfl_sync(FULL_MASK, ok, 0);
-      if (!ok) return;  // reported; this tile is left unsolved
-      __syncwarp();
+    R f, l;
+    reduced_solve<R>(t2, b2, lane, 32, f, l, bad);
+    if (lane < K) {
+      p.tile_fl[2 * (ts + lane)] = f;
+      p.tile_fl[2 * (ts + lane) + 1] = l;
     }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0 && !p.withhold) atomicExch(&p.sys_ready[s], 1u);
     const R xp = j > 0 ? __ldcg(p.tile_fl + 2 * (ts + j - 1) + 1) : R(0);
     const R xn = j < K - 1 ? __ldcg(p.tile_fl + 2 * (ts + j + 1)) : R(0);
-    yy = y[0] + y[1] * xp + y[2] * xn;
-    zz = z[0] + z[1] * xp + z[2] * xn;
+    tile_store<R>(p, base0 + r0, nt, a, c, d, y[0] + y[1] * xp + y[2] * xn, z[0] + z[1] * xp + z[2] * xn,
+                  buf, lane);
+    return false;
   }
-  chunk_substitute<R, kTM>(a, c, d, yy, zz);
-  // x out through the warp's d rows, then coalesced element stores
-  sts_row<R, kTM>(buf + 3 * L::BUF + lane * L::ROW, d);
+  // to park: interior rows' a', c', d', then y, z
+#pragma unroll
+  for (int i = 1; i < kTM - 1; ++i) {
+    pw.put(i - 1, a[i]);
+    pw.put(kTM - 2 + i - 1, c[i]);
+    pw.put(2 * (kTM - 2) + i - 1, d[i]);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    pw.put(3 * (kTM - 2) + k, y[k]);
+    pw.put(3 * (kTM - 2) + 3 + k, z[k]);
+  }
+  return true;
+}
+
+// Parking slot transfers (three 32-column blocks). park_swap stores the new
+// tile's words block by block in place of the parked tile's, which it
+// returns in the same array, so at most one block of extra registers is live.
+template <typename R> __device__ __forceinline__ void park_put(uint32_t slot, const ParkWords<R> &pw) {
+  tmem_put(slot + 0, pw.w[0]);
+  tmem_put(slot + 32, pw.w[1]);
+  tmem_put(slot + 64, pw.w[2]);
+  tmem_wait_st();
+}
+template <typename R> __device__ __forceinline__ void park_get(uint32_t slot, ParkWords<R> &pw) {
+  tmem_get(slot + 0, pw.w[0]);
+  tmem_get(slot + 32, pw.w[1]);
+  tmem_get(slot + 64, pw.w[2]);
+  tmem_wait_ld(pw.w[0]);
+  tmem_wait_ld(pw.w[1]);
+  tmem_wait_ld(pw.w[2]);
+}
+template <typename R> __device__ __forceinline__ void park_swap(uint32_t slot, ParkWords<R> &pw) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    uint32_t v[16], o[16];
+    tmem_get(slot + 16 * k, v);
+    tmem_wait_ld(v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) o[i] = pw.w[k / 2][16 * (k % 2) + i];
+    tmem_put(slot + 16 * k, o);
+    tmem_wait_st();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) pw.w[k / 2][16 * (k % 2) + i] = v[i];
+  }
+}
+
+// Tile item, second part: waits (bounded) for the parked tile's system to
+// publish its second-level solution, then substitutes (the tile's words in
+// pw) and stores.
+template <typename R>
+__device__ __forceinline__ void tile_finish(const RaggedArgs<R> &p, long long item,
+                                            const ParkWords<R> &pw, R *buf, int lane) {
+  // the parked tile's place, read again (L2) rather than held in registers
+  const int4 meta = p.tile_meta[item];
+  const int s = meta.x;
+  const int j = meta.y;
+  const int K = meta.z;
+  const long long ts = item - j;
+  const long long r0 = (long long)j * tile_rows<R>();
+  const long long base = p.tile_base[item] + r0;
+  const int nt = (int)(meta.w - r0 < tile_rows<R>() ? meta.w - r0 : tile_rows<R>());
+  unsigned ok = 1;
+  if (lane == 0) {
+    // bounded: p.wait_limit polls (kWaitLimit unless a test lowered it), and
+    // none at all once any wait of this launch has given up (error != 0)
+    const volatile unsigned *err = p.error;
+    unsigned it = 0;
+    unsigned r = load_acquire(p.sys_ready + s);
+    while (r == 0u && *err == 0u && it < p.wait_limit) {
+      __nanosleep(128);
+      ++it;
+      r = load_acquire(p.sys_ready + s);
+    }
+    ok = r != 0u;
+    if (!ok) atomicExch(p.error, 2u);
+  }
+  ok = __shfl_sync(FULL_MASK, ok, 0);
+  if (!ok) return;  // reported; this tile is left unsolved
+  __syncwarp();
+  using L = SmemLayout<R, tile_m<R>()>;
+  constexpr int kTM = tile_m<R>();
+  constexpr int I0 = 3 * (kTM - 2);  // y[3], z[3] follow the rows
+  const R xp = j > 0 ? __ldcg(p.tile_fl + 2 * (ts + j - 1) + 1) : R(0);
+  const R xn = j < K - 1 ? __ldcg(p.tile_fl + 2 * (ts + j + 1)) : R(0);
+  const R yy = pw.get(I0 + 0) + pw.get(I0 + 1) * xp + pw.get(I0 + 2) * xn;
+  const R zz = pw.get(I0 + 3) + pw.get(I0 + 4) * xp + pw.get(I0 + 5) * xn;
+  // x_i = d'_i - a'_i x_first - c'_i x_last (x_first = yy, x_last = zz),
+  // straight from the parked words into the lane's staged row, 16 bytes at
+  // a time
+  using Vt = typename Vec16<R>::T;
+  constexpr int n = Vec16<R>::n;
+  Vt *row = reinterpret_cast<Vt *>(buf + 3 * L::BUF + lane * L::ROW);
+#pragma unroll
+  for (int g = 0; g < kTM / n; ++g) {
+    R x[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      const int i = g * n + k;
+      if (i == 0)
+        x[k] = yy;
+      else if (i == kTM - 1)
+        x[k] = zz;
+      else
+        x[k] = pw.get(2 * (kTM - 2) + i - 1) - pw.get(i - 1) * yy - pw.get(kTM - 2 + i - 1) * zz;
+    }
+    Vt v;
+    if constexpr (n == 2) {
+      v.x = x[0];
+      v.y = x[1];
+    } else {
+      v.x = x[0];
+      v.y = x[1];
+      v.z = x[2];
+      v.w = x[3];
+    }
+    row[g] = v;
+  }
   __syncwarp();
 #pragma unroll 4
-  for (int e = lane; e < nt; e += 32) p.d[base0 + r0 + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
+  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
   __syncwarp();  // the buffer is free for the next item
 }
 
+// Persistent warps take tile items (longest systems first), then warp items,
+// from one global counter. A warp holds at most one parked tile, in its TMEM
+// slot: after the first part of each new tile it swaps the new tile in and
+// finishes the one parked before (after a warp item, or a tile finished at
+// once, it takes the parked one out and finishes it), so each wait has had
+// a whole item of slack.
 template <typename R>
-__global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs<R> p) {
+__global__ void __launch_bounds__(kRaggedThreads, 3) ragged_kernel(const RaggedArgs<R> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t tmem_slot;
   const int lane = threadIdx.x & 31;
-  R *buf = reinterpret_cast<R *>(smem_raw) + (threadIdx.x >> 5) * TileBuf<R>::ELEMS;
-  if (*reinterpret_cast<volatile unsigned *>(p.error) == 3u) return;  // tile table refused
+  const int warp = threadIdx.x >> 5;
+  R *buf = reinterpret_cast<R *>(smem_raw) + warp * TileBuf<R>::ELEMS;
+  if (*reinterpret_cast<volatile unsigned *>(p.error) == 3u) return;  // tile table refused (uniform)
+  if (warp == 0) tmem_alloc_cols<kRaggedTmemCols>(&tmem_slot);
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t tbase = tmem_slot;
+  const uint32_t slot = tbase + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter
   long long ntiles = 0, nwarp = 0;
   for (int c = 0; c < kClasses; ++c) {
     if (p.mtab[c] == 0)
@@ -311,6 +480,8 @@ __global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs
       nwarp += p.hist[c];
   }
   bool bad = false;
+  bool parked = false;
+  long long pk = 0;  // the parked tile's item
   for (;;) {
     long long it = 0;
     if (lane == 0) it = (long long)atomicAdd(p.counter, 1ULL);
@@ -321,25 +492,75 @@ __global__ void __launch_bounds__(kRaggedThreads) ragged_kernel(const RaggedArgs
         if (lane == 0 && meta.y == 0) atomicExch(p.error, 1u);
         continue;
       }
-      tile_item<R>(p, it, buf, lane, bad);
+      ParkWords<R> pw;
+      if (tile_publish<R>(p, it, buf, lane, pw, bad)) {
+        if (parked) {
+          park_swap<R>(slot, pw);  // the new tile in, the parked one out (into pw)
+          tile_finish<R>(p, pk, pw, buf, lane);
+        } else {
+          park_put<R>(slot, pw);
+        }
+        pk = it;
+        parked = true;
+      } else if (parked) {
+        park_get<R>(slot, pw);
+        tile_finish<R>(p, pk, pw, buf, lane);
+        parked = false;
+      }
       continue;
     }
     it -= ntiles;
-    if (it >= nwarp) break;
-    const int s = p.order[it];
-    const long long base = p.off[s];
-    const long long n = p.off[s + 1] - base;
-    switch (p.mtab[length_class(n > 0 ? n : 1)]) {
-      case 1: warp_item<R, 1>(p, base, n, lane, bad); break;
-      case 2: warp_item<R, 2>(p, base, n, lane, bad); break;
-      case 4: warp_item<R, 4>(p, base, n, lane, bad); break;
-      default: warp_item<R, 8>(p, base, n, lane, bad); break;
+    if (it < nwarp) {
+      const int s = p.order[it];
+      const long long base = p.off[s];
+      const long long n = p.off[s + 1] - base;
+      switch (p.mtab[length_class(n > 0 ? n : 1)]) {
+        case 1: warp_item<R, 1>(p, base, n, lane, bad); break;
+        case 2: warp_item<R, 2>(p, base, n, lane, bad); break;
+        case 4: warp_item<R, 4>(p, base, n, lane, bad); break;
+        default: warp_item<R, 8>(p, base, n, lane, bad); break;
+      }
     }
+    if (parked) {
+      ParkWords<R> pw;
+      park_get<R>(slot, pw);
+      tile_finish<R>(p, pk, pw, buf, lane);
+      parked = false;
+    }
+    if (it >= nwarp) break;
   }
   report_bad_pivot(bad, p.flag);
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (warp == 0) tmem_dealloc_cols<kRaggedTmemCols>(tbase);
 }
 
 // ---- host side ---------------------------------------------------------------
+
+// Resident CTAs per SM of the ragged kernel (at least 1): the smallest of
+// the shared-memory, register and TMEM-column limits. (Were fewer resident,
+// the extra CTAs would start as others exit and find the items taken: every
+// claimed tile is published before its warp waits on anything.)
+template <typename K>
+static int ragged_ctas_per_sm(int dev, K kernel, size_t smem) {
+  int smem_sm = 0, reserved = 0, regs_sm = 0;
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  const long long per_cta_smem = (long long)smem + (long long)fa.sharedSizeBytes + reserved;
+  const long long warp_regs = ((long long)fa.numRegs * 32 + 255) / 256 * 256;  // allocated per warp
+  const long long per_cta_regs = warp_regs * (kRaggedThreads / 32);
+  long long n = 512 / kRaggedTmemCols;
+  if (per_cta_smem > 0 && smem_sm / per_cta_smem < n) n = smem_sm / per_cta_smem;
+  if (per_cta_regs > 0 && regs_sm / per_cta_regs < n) n = regs_sm / per_cta_regs;
+  return n < 1 ? 1 : (int)n;
+}
 
 // Rows per lane by length class: M > 0 for warp items, 0 for tile classes.
 // Built-in table, replaced per device and precision by tridRaggedAutotune.
@@ -461,13 +682,15 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
+    // (73.7 KB: three CTAs per SM, 3 x 128 TMEM columns)
     const size_t smem = (size_t)(kRaggedThreads / 32) * TileBuf<R>::ELEMS * sizeof(R);
-    cudaFuncSetAttribute(ragged_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ragged_kernel<R>, kRaggedThreads, smem);
-    if (per_sm < 1) per_sm = 1;
+    e = cudaFuncSetAttribute(ragged_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // CTAs per SM from the shared memory, registers and TMEM columns a CTA
+    // takes (the runtime's occupancy query answers one CTA per SM for this
+    // kernel, counting it as if it held all 512 TMEM columns)
+    int per_sm = ragged_ctas_per_sm(dev, ragged_kernel<R>, smem);
     // every CTA resident at once (the waits rely on running warps only)
-    ragged_kernel<R><<<(unsigned)(sms * per_sm), kRaggedThreads, smem, st>>>(p);
+    if (e == cudaSuccess) ragged_kernel<R><<<(unsigned)(sms * per_sm), kRaggedThreads, smem, st>>>(p);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     e = cudaGetLastError();
   }

@@ -50,6 +50,7 @@
 #include <type_traits>
 
 #include "trid_internal.h"
+#include "trid_tmem.cuh"
 
 namespace trid {
 
@@ -70,28 +71,6 @@ constexpr int WIDE_SMEM_MIN = 120 * 1024;  // one CTA per SM
 constexpr int WIDE2_SMEM_MIN = 80 * 1024;
 constexpr int WIDE2_SMEM_MAX = 112 * 1024;
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// NCOL columns (a power of two, 32..512) for the CTA
-template <int NCOL> __device__ __forceinline__ void tmem_alloc_cols(uint32_t *slot) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot)),
-               "n"(NCOL)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-}
-template <int NCOL> __device__ __forceinline__ void tmem_dealloc_cols(uint32_t base) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(base), "n"(NCOL) : "memory");
-}
-__device__ __forceinline__ void tmem_fence_before_sync() {
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_after_sync() {
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
-
 // one row's a', c' (of the thread's S systems) into its lane at column taddr
 template <typename R, int S>
 __device__ __forceinline__ void tmem_put_row(uint32_t taddr, const R (&af)[S], const R (&cf)[S]) {
@@ -108,46 +87,6 @@ __device__ __forceinline__ void tmem_put_row(uint32_t taddr, const R (&af)[S], c
                  "r"(__float_as_uint(cf[1]))
                  : "memory");
   }
-}
-
-// 16 or 32 consecutive columns of this thread's lane (then tmem_wait_ld)
-__device__ __forceinline__ void tmem_get(uint32_t taddr, uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-      "[%32];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-        "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-        "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-        "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-      : "r"(taddr)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_get(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-      "%13, %14, %15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-        "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
-}
-
-// Waits for this thread's TMEM loads. The loaded registers are in/out
-// operands, so no use of them can be scheduled above the wait.
-__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
-               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
-               :
-               : "memory");
-}
-__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[16]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
-               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
-               :
-               : "memory");
 }
 
 // a', c' of row i, system q of a block loaded by tmem_get (4 columns a row)

@@ -89,6 +89,49 @@ __device__ __forceinline__ void reduced_solve3(const Row<R> &top, const Row<R> &
   }
 }
 
+// chunk_forward (reciprocal estimates) with the diagonal read from the
+// lane's staged row `brow` 16 bytes at a time as the sweep needs it, so b
+// takes no registers beyond one vector.
+template <typename R, int M>
+__device__ __forceinline__ void chunk_forward_staged(R (&a)[M], const R *brow, R (&c)[M], R (&d)[M],
+                                                     bool &bad) {
+  using Vt = typename Vec16<R>::T;
+  constexpr int n = Vec16<R>::n;
+  static_assert(M % n == 0 && M >= 2, "whole vectors");
+  const Vt *q = reinterpret_cast<const Vt *>(brow);
+#pragma unroll
+  for (int g = 0; g < M / n; ++g) {
+    const Vt v = q[g];
+    R bv[n];
+    if constexpr (n == 2) {
+      bv[0] = v.x;
+      bv[1] = v.y;
+    } else {
+      bv[0] = v.x;
+      bv[1] = v.y;
+      bv[2] = v.z;
+      bv[3] = v.w;
+    }
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      const int i = g * n + k;
+      if (i < 2) {
+        const R r = rcp_nr(bv[k]);
+        bad |= !finite_rcp(r);
+        a[i] *= r;
+        c[i] *= r;
+        d[i] *= r;
+      } else {
+        const R r = rcp_nr(bv[k] - a[i] * c[i - 1]);
+        bad |= !finite_rcp(r);
+        d[i] = r * (d[i] - a[i] * d[i - 1]);
+        a[i] = -r * a[i] * a[i - 1];
+        c[i] = r * c[i];
+      }
+    }
+  }
+}
+
 // Shared memory of one warp's tile: a, b, c, d in padded chunk rows (as
 // contig_smem_kernel), d's rows reused for x on the way out.
 template <typename R> struct TileBuf {
