@@ -5,13 +5,13 @@
 //   1. ragged_hist_kernel / ragged_order_kernel bucket the systems by length
 //      class (ceil(log2 N)), longest class first (longest-processing-time
 //      order keeps the SMs evenly loaded at the end). A system of a "tile"
-//      class is cut into K tiles of 512 rows (FP64; 1024 rows FP32) and each tile
-//      becomes one work item; a system of a "warp" class (short systems,
+//      class is cut into K tiles of 512 rows and each tile becomes one work
+//      item; a system of a "warp" class (short systems,
 //      rows-per-lane M from the class table) is one warp item;
 //   2. ragged_kernel: persistent warps take tile items (longest systems
 //      first), then warp items, from one global counter.
 //
-// Tile item (one warp, 16 rows per lane FP64, 32 FP32): the warp stages the tile's rows of
+// Tile item (one warp, 16 rows per lane): the warp stages the tile's rows of
 // a, b, c, d in shared memory with coalesced cp.async copies, each lane runs
 // the chunk elimination on its 16 rows, and the warp's reduced solve is run
 // for three right-hand sides at once: the tile's own, and the unit
@@ -20,16 +20,18 @@
 // reduced unknown of the tile is then p + alpha x_prev + beta x_next. From
 // the tile's first and last unknowns the warp forms the tile's two rows of
 // a second-level tridiagonal system (2 rows per tile, at most 64 rows), and
-// the warp that finishes the last tile of a system solves it with one warp
-// PCR and publishes every tile's first and last unknown. The other warps of
+// the warp that finishes the last tile of a system solves it (two tiles a
+// lane, then one warp PCR) and publishes every tile's first and last
+// unknown. The other warps of
 // the system park their tile's eliminated rows in tensor memory (96 32-bit
-// columns of the warp's lane quarter), take their next item, and only after
+// columns FP64, 48 FP32, of the warp's lane quarter), take their next item,
+// and only after
 // publishing that one (or after a warp item) wait (bounded, on a flag) for
 // the parked tile's system, then substitute and store. So every element is
 // read once and written once, with 8 values of scratch per tile, and a wait
 // has a whole item of slack (the earlier form held the tile in registers and
 // waited at once: 17 us a wait on average, a third of the warps' time).
-// A warp holds at most one parked tile, in one of its two TMEM slots; each
+// A warp holds at most one parked tile, in its TMEM slot; each
 // claimed tile is published before its warp waits on anything, and claims
 // are in system order, so the tiles a warp waits for are held by running
 // warps: the wait always ends.
@@ -52,7 +54,17 @@ namespace trid {
 constexpr int kClasses = 24;        // length classes 0..23: N <= 2^class
 // Tile items (tile_m / tile_rows, trid_tile.cuh): tiles per system, N <=
 // 16384 either way, so the second-level system has at most 64 rows.
-template <typename R> constexpr int max_tiles() { return 16384 / tile_rows<R>(); }
+// Ragged tiles: 16 rows per lane, 512 rows, in both precisions (measured on
+// the 200k-system batch against 8 FP64 / 32 FP32 rows a lane: FP64 4.69 vs
+// 5.20 ms, FP32 2.85 vs 2.98 ms). An FP32 lane's eliminated rows then take
+// half the registers and a tile half the TMEM columns of an FP64 one, so
+// four FP32 CTAs of 4 warps fit an SM against three FP64 ones; at most 32
+// tiles a system of 16384 rows.
+template <typename R> constexpr int rtile_m() { return 16; }
+template <typename R> constexpr int ragged_ctas() { return sizeof(R) == 8 ? 3 : 4; }
+template <typename R> constexpr int rtile_rows() { return 32 * rtile_m<R>(); }
+template <typename R> using RTileBuf = TileBuf<R, rtile_m<R>()>;
+template <typename R> constexpr int max_tiles() { return 16384 / rtile_rows<R>(); }
 constexpr int kRaggedThreads = 128; // 4 warps per CTA
 constexpr unsigned kWaitLimit = 1u << 22;  // polls of the ready flag (each with a short sleep)
 
@@ -108,7 +120,7 @@ __global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist, unsigned lon
     const long long n = p.off[s + 1] - p.off[s];
     const int c = length_class(n > 0 ? n : 1);
     atomicAdd(&hist[c], 1u);
-    if (p.mtab[c] == 0) atomicAdd(&tiles[c], (unsigned long long)((n + tile_rows<R>() - 1) / tile_rows<R>()));
+    if (p.mtab[c] == 0) atomicAdd(&tiles[c], (unsigned long long)((n + rtile_rows<R>() - 1) / rtile_rows<R>()));
   }
 }
 
@@ -125,7 +137,7 @@ __global__ void ragged_order_kernel(RaggedArgs<R> p, const unsigned *hist,
       unsigned long long t0 = 0;
       for (int q = kClasses - 1; q > c; --q)
         if (p.mtab[q] == 0) t0 += tiles[q];
-      const long long K = (n + tile_rows<R>() - 1) / tile_rows<R>();
+      const long long K = (n + rtile_rows<R>() - 1) / rtile_rows<R>();
       const long long ts = (long long)(t0 + atomicAdd(&tfill[c], (unsigned long long)K));
       if (ts + K > p.max_tiles) {  // offsets not ascending: refuse rather than overrun
         atomicExch(p.error, 3u);
@@ -199,30 +211,30 @@ __device__ __forceinline__ void warp_item(const RaggedArgs<R> &p, long long base
 }
 
 
-// TMEM per CTA: one parking slot in each warp's lane quarter, 96 columns
-// (a', c', d' of the lane's interior rows 1 .. M-2 and the reduced solve's
-// y[3], z[3], as 32-bit words) of the CTA's 128.
-constexpr int kRaggedTmemCols = 128;
+// TMEM per CTA: one parking slot in each warp's lane quarter: a', c', d' of
+// the lane's interior rows 1 .. M-2 and the reduced solve's y[3], z[3], as
+// 32-bit words (96 columns FP64, 48 FP32, of the CTA's 128 or 64).
+template <typename R> constexpr int park_words() { return (sizeof(R) / 4) * (3 * (rtile_m<R>() - 2) + 6); }
+template <typename R> constexpr int ragged_tmem_cols() { return park_words<R>() <= 64 ? 64 : 128; }
+static_assert(park_words<double>() % 16 == 0 && park_words<float>() % 16 == 0, "16-column transfers");
 
-template <typename R> constexpr int park_words() { return (sizeof(R) / 4) * (3 * (tile_m<R>() - 2) + 6); }
-static_assert(park_words<double>() == 96 && park_words<float>() == 96, "three 32-column transfers");
-
-// The values of a parked tile, one 32-bit word array per 32 columns.
+// The values of a parked tile, one 32-bit word array per 16 columns.
 template <typename R> struct ParkWords {
-  uint32_t w[3][32];
+  static constexpr int NB = park_words<R>() / 16;
+  uint32_t w[NB][16];
   __device__ __forceinline__ void put(int k, R v) {
     if constexpr (sizeof(R) == 8) {
-      w[(2 * k) / 32][(2 * k) % 32] = (uint32_t)__double2loint(v);
-      w[(2 * k + 1) / 32][(2 * k + 1) % 32] = (uint32_t)__double2hiint(v);
+      w[(2 * k) / 16][(2 * k) % 16] = (uint32_t)__double2loint(v);
+      w[(2 * k + 1) / 16][(2 * k + 1) % 16] = (uint32_t)__double2hiint(v);
     } else {
-      w[k / 32][k % 32] = __float_as_uint(v);
+      w[k / 16][k % 16] = __float_as_uint(v);
     }
   }
   __device__ __forceinline__ R get(int k) const {
     if constexpr (sizeof(R) == 8)
-      return __hiloint2double((int)w[(2 * k + 1) / 32][(2 * k + 1) % 32], (int)w[(2 * k) / 32][(2 * k) % 32]);
+      return __hiloint2double((int)w[(2 * k + 1) / 16][(2 * k + 1) % 16], (int)w[(2 * k) / 16][(2 * k) % 16]);
     else
-      return __uint_as_float(w[k / 32][k % 32]);
+      return __uint_as_float(w[k / 16][k % 16]);
   }
 };
 
@@ -231,14 +243,14 @@ template <typename R> struct ParkWords {
 // the warp's d rows with coalesced element stores.
 template <typename R>
 __device__ __forceinline__ void tile_store(const RaggedArgs<R> &p, long long base, int nt,
-                                           R (&a)[tile_m<R>()], R (&c)[tile_m<R>()],
-                                           R (&d)[tile_m<R>()], R yy, R zz, R *buf, int lane) {
-  using L = SmemLayout<R, tile_m<R>()>;
-  chunk_substitute<R, tile_m<R>()>(a, c, d, yy, zz);
-  sts_row<R, tile_m<R>()>(buf + 3 * L::BUF + lane * L::ROW, d);
+                                           R (&a)[rtile_m<R>()], R (&c)[rtile_m<R>()],
+                                           R (&d)[rtile_m<R>()], R yy, R zz, R *buf, int lane) {
+  using L = SmemLayout<R, rtile_m<R>()>;
+  chunk_substitute<R, rtile_m<R>()>(a, c, d, yy, zz);
+  sts_row<R, rtile_m<R>()>(buf + 3 * L::BUF + lane * L::ROW, d);
   __syncwarp();
 #pragma unroll 4
-  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
+  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + RTileBuf<R>::slot(e)];
   __syncwarp();  // the buffer is free for the next item
 }
 
@@ -253,7 +265,7 @@ __device__ __forceinline__ void tile_store(const RaggedArgs<R> &p, long long bas
 template <typename R>
 __device__ __forceinline__ bool tile_publish(const RaggedArgs<R> &p, long long item, R *buf, int lane,
                                              ParkWords<R> &pw, bool &bad) {
-  using L = SmemLayout<R, tile_m<R>()>;
+  using L = SmemLayout<R, rtile_m<R>()>;
   const int4 meta = p.tile_meta[item];
   const int s = meta.x;
   const int j = meta.y;
@@ -261,11 +273,11 @@ __device__ __forceinline__ bool tile_publish(const RaggedArgs<R> &p, long long i
   const long long n = meta.w;
   const long long ts = item - j;
   const long long base0 = p.tile_base[item];
-  const long long r0 = (long long)j * tile_rows<R>();
-  const int nt = (int)(n - r0 < tile_rows<R>() ? n - r0 : tile_rows<R>());
-  stage_tile_rows<R>(p.a, p.b, p.c, p.d, p.vec16, base0 + r0, nt, buf, lane);
+  const long long r0 = (long long)j * rtile_rows<R>();
+  const int nt = (int)(n - r0 < rtile_rows<R>() ? n - r0 : rtile_rows<R>());
+  stage_tile_rows<R, rtile_m<R>()>(p.a, p.b, p.c, p.d, p.vec16, base0 + r0, nt, buf, lane);
 
-  constexpr int kTM = tile_m<R>();
+  constexpr int kTM = rtile_m<R>();
   R a[kTM], c[kTM], d[kTM];
   lds_row<R, kTM>(buf + 0 * L::BUF + lane * L::ROW, a);
   lds_row<R, kTM>(buf + 2 * L::BUF + lane * L::ROW, c);
@@ -307,17 +319,37 @@ __device__ __forceinline__ bool tile_publish(const RaggedArgs<R> &p, long long i
   last = __shfl_sync(FULL_MASK, last, 0);
   if (last) {
     __syncwarp();
-    Row<R> t2{R(0), R(0), R(0)}, b2{R(0), R(0), R(0)};
-    if (lane < K) {
-      const R *tr = p.tile_rows + 6 * (ts + lane);  // read from L2, not a stale L1 line
-      t2 = Row<R>{__ldcg(tr + 0), __ldcg(tr + 1), __ldcg(tr + 2)};
-      b2 = Row<R>{__ldcg(tr + 3), __ldcg(tr + 4), __ldcg(tr + 5)};
+    // the second-level system, rows f_0, l_0, f_1, l_1, ... (2 a tile, up
+    // to 128): two tiles (4 rows, unit diagonal) a lane, identity rows past
+    // the last tile
+    R qa[4], qb[4], qc[4], qd[4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = 2 * lane + h;
+      qb[2 * h] = qb[2 * h + 1] = R(1);
+      qa[2 * h] = qc[2 * h] = qd[2 * h] = qa[2 * h + 1] = qc[2 * h + 1] = qd[2 * h + 1] = R(0);
+      if (t < K) {
+        const R *tr = p.tile_rows + 6 * (ts + t);  // read from L2, not a stale L1 line
+        qa[2 * h] = __ldcg(tr + 0);
+        qc[2 * h] = __ldcg(tr + 1);
+        qd[2 * h] = __ldcg(tr + 2);
+        qa[2 * h + 1] = __ldcg(tr + 3);
+        qc[2 * h + 1] = __ldcg(tr + 4);
+        qd[2 * h + 1] = __ldcg(tr + 5);
+      }
     }
+    chunk_forward<R, 4>(qa, qb, qc, qd, bad);
+    chunk_backward<R, 4>(qa, qc, qd, bad);
     R f, l;
-    reduced_solve<R>(t2, b2, lane, 32, f, l, bad);
-    if (lane < K) {
-      p.tile_fl[2 * (ts + lane)] = f;
-      p.tile_fl[2 * (ts + lane) + 1] = l;
+    reduced_solve<R>(Row<R>{qa[0], qc[0], qd[0]}, Row<R>{qa[3], qc[3], qd[3]}, lane, 32, f, l, bad);
+    chunk_substitute<R, 4>(qa, qc, qd, f, l);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = 2 * lane + h;
+      if (t < K) {
+        p.tile_fl[2 * (ts + t)] = qd[2 * h];
+        p.tile_fl[2 * (ts + t) + 1] = qd[2 * h + 1];
+      }
     }
     __threadfence();
     __syncwarp();
@@ -343,35 +375,30 @@ __device__ __forceinline__ bool tile_publish(const RaggedArgs<R> &p, long long i
   return true;
 }
 
-// Parking slot transfers (three 32-column blocks). park_swap stores the new
+// Parking slot transfers (16-column blocks). park_swap stores the new
 // tile's words block by block in place of the parked tile's, which it
 // returns in the same array, so at most one block of extra registers is live.
 template <typename R> __device__ __forceinline__ void park_put(uint32_t slot, const ParkWords<R> &pw) {
-  tmem_put(slot + 0, pw.w[0]);
-  tmem_put(slot + 32, pw.w[1]);
-  tmem_put(slot + 64, pw.w[2]);
+#pragma unroll
+  for (int k = 0; k < ParkWords<R>::NB; ++k) tmem_put(slot + 16 * k, pw.w[k]);
   tmem_wait_st();
 }
 template <typename R> __device__ __forceinline__ void park_get(uint32_t slot, ParkWords<R> &pw) {
-  tmem_get(slot + 0, pw.w[0]);
-  tmem_get(slot + 32, pw.w[1]);
-  tmem_get(slot + 64, pw.w[2]);
-  tmem_wait_ld(pw.w[0]);
-  tmem_wait_ld(pw.w[1]);
-  tmem_wait_ld(pw.w[2]);
+#pragma unroll
+  for (int k = 0; k < ParkWords<R>::NB; ++k) tmem_get(slot + 16 * k, pw.w[k]);
+#pragma unroll
+  for (int k = 0; k < ParkWords<R>::NB; ++k) tmem_wait_ld(pw.w[k]);
 }
 template <typename R> __device__ __forceinline__ void park_swap(uint32_t slot, ParkWords<R> &pw) {
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    uint32_t v[16], o[16];
+  for (int k = 0; k < ParkWords<R>::NB; ++k) {
+    uint32_t v[16];
     tmem_get(slot + 16 * k, v);
     tmem_wait_ld(v);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) o[i] = pw.w[k / 2][16 * (k % 2) + i];
-    tmem_put(slot + 16 * k, o);
+    tmem_put(slot + 16 * k, pw.w[k]);
     tmem_wait_st();
 #pragma unroll
-    for (int i = 0; i < 16; ++i) pw.w[k / 2][16 * (k % 2) + i] = v[i];
+    for (int i = 0; i < 16; ++i) pw.w[k][i] = v[i];
   }
 }
 
@@ -387,9 +414,9 @@ __device__ __forceinline__ void tile_finish(const RaggedArgs<R> &p, long long it
   const int j = meta.y;
   const int K = meta.z;
   const long long ts = item - j;
-  const long long r0 = (long long)j * tile_rows<R>();
+  const long long r0 = (long long)j * rtile_rows<R>();
   const long long base = p.tile_base[item] + r0;
-  const int nt = (int)(meta.w - r0 < tile_rows<R>() ? meta.w - r0 : tile_rows<R>());
+  const int nt = (int)(meta.w - r0 < rtile_rows<R>() ? meta.w - r0 : rtile_rows<R>());
   unsigned ok = 1;
   if (lane == 0) {
     // bounded: p.wait_limit polls (kWaitLimit unless a test lowered it), and
@@ -408,8 +435,8 @@ __device__ __forceinline__ void tile_finish(const RaggedArgs<R> &p, long long it
   ok = __shfl_sync(FULL_MASK, ok, 0);
   if (!ok) return;  // reported; this tile is left unsolved
   __syncwarp();
-  using L = SmemLayout<R, tile_m<R>()>;
-  constexpr int kTM = tile_m<R>();
+  using L = SmemLayout<R, rtile_m<R>()>;
+  constexpr int kTM = rtile_m<R>();
   constexpr int I0 = 3 * (kTM - 2);  // y[3], z[3] follow the rows
   const R xp = j > 0 ? __ldcg(p.tile_fl + 2 * (ts + j - 1) + 1) : R(0);
   const R xn = j < K - 1 ? __ldcg(p.tile_fl + 2 * (ts + j + 1)) : R(0);
@@ -448,7 +475,7 @@ __device__ __forceinline__ void tile_finish(const RaggedArgs<R> &p, long long it
   }
   __syncwarp();
 #pragma unroll 4
-  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + TileBuf<R>::slot(e)];
+  for (int e = lane; e < nt; e += 32) p.d[base + e] = buf[3 * L::BUF + RTileBuf<R>::slot(e)];
   __syncwarp();  // the buffer is free for the next item
 }
 
@@ -459,14 +486,14 @@ __device__ __forceinline__ void tile_finish(const RaggedArgs<R> &p, long long it
 // once, it takes the parked one out and finishes it), so each wait has had
 // a whole item of slack.
 template <typename R>
-__global__ void __launch_bounds__(kRaggedThreads, 3) ragged_kernel(const RaggedArgs<R> p) {
+__global__ void __launch_bounds__(kRaggedThreads, ragged_ctas<R>()) ragged_kernel(const RaggedArgs<R> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t tmem_slot;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  R *buf = reinterpret_cast<R *>(smem_raw) + warp * TileBuf<R>::ELEMS;
+  R *buf = reinterpret_cast<R *>(smem_raw) + warp * RTileBuf<R>::ELEMS;
   if (*reinterpret_cast<volatile unsigned *>(p.error) == 3u) return;  // tile table refused (uniform)
-  if (warp == 0) tmem_alloc_cols<kRaggedTmemCols>(&tmem_slot);
+  if (warp == 0) tmem_alloc_cols<ragged_tmem_cols<R>()>(&tmem_slot);
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
@@ -533,7 +560,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 3) ragged_kernel(const RaggedA
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
-  if (warp == 0) tmem_dealloc_cols<kRaggedTmemCols>(tbase);
+  if (warp == 0) tmem_dealloc_cols<ragged_tmem_cols<R>()>(tbase);
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -543,7 +570,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 3) ragged_kernel(const RaggedA
 // the extra CTAs would start as others exit and find the items taken: every
 // claimed tile is published before its warp waits on anything.)
 template <typename K>
-static int ragged_ctas_per_sm(int dev, K kernel, size_t smem) {
+static int ragged_ctas_per_sm(int dev, K kernel, size_t smem, int tmem_cols) {
   int smem_sm = 0, reserved = 0, regs_sm = 0;
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
@@ -556,7 +583,7 @@ static int ragged_ctas_per_sm(int dev, K kernel, size_t smem) {
   const long long per_cta_smem = (long long)smem + (long long)fa.sharedSizeBytes + reserved;
   const long long warp_regs = ((long long)fa.numRegs * 32 + 255) / 256 * 256;  // allocated per warp
   const long long per_cta_regs = warp_regs * (kRaggedThreads / 32);
-  long long n = 512 / kRaggedTmemCols;
+  long long n = 512 / tmem_cols;
   if (per_cta_smem > 0 && smem_sm / per_cta_smem < n) n = smem_sm / per_cta_smem;
   if (per_cta_regs > 0 && regs_sm / per_cta_regs < n) n = regs_sm / per_cta_regs;
   return n < 1 ? 1 : (int)n;
@@ -617,7 +644,7 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   if (e != cudaSuccess) return e;
   const long long elems = ends[1] - ends[0];
   if (elems < 0) return cudaErrorInvalidValue;
-  const long long max_tiles = elems / tile_rows<R>() + p.nsys + 1;
+  const long long max_tiles = elems / rtile_rows<R>() + p.nsys + 1;
   // scratch: header | order (int, nsys) | done, ready (u32, nsys each) |
   // tile_meta (int4, max_tiles) | tile_base (i64) | tile_rows (6 R) | tile_fl (2 R)
   // header: hist u32[24] @0, fill u32[24] @128, tiles u64[24] @256,
@@ -683,12 +710,12 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   }
   if (e == cudaSuccess) {
     // (73.7 KB: three CTAs per SM, 3 x 128 TMEM columns)
-    const size_t smem = (size_t)(kRaggedThreads / 32) * TileBuf<R>::ELEMS * sizeof(R);
+    const size_t smem = (size_t)(kRaggedThreads / 32) * RTileBuf<R>::ELEMS * sizeof(R);
     e = cudaFuncSetAttribute(ragged_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // CTAs per SM from the shared memory, registers and TMEM columns a CTA
     // takes (the runtime's occupancy query answers one CTA per SM for this
     // kernel, counting it as if it held all 512 TMEM columns)
-    int per_sm = ragged_ctas_per_sm(dev, ragged_kernel<R>, smem);
+    int per_sm = ragged_ctas_per_sm(dev, ragged_kernel<R>, smem, ragged_tmem_cols<R>());
     // every CTA resident at once (the waits rely on running warps only)
     if (e == cudaSuccess) ragged_kernel<R><<<(unsigned)(sms * per_sm), kRaggedThreads, smem, st>>>(p);
     g_launches.fetch_add(1, std::memory_order_relaxed);

@@ -134,10 +134,11 @@ __device__ __forceinline__ void chunk_forward_staged(R (&a)[M], const R *brow, R
 
 // Shared memory of one warp's tile: a, b, c, d in padded chunk rows (as
 // contig_smem_kernel), d's rows reused for x on the way out.
-template <typename R> struct TileBuf {
-  using L = SmemLayout<R, tile_m<R>()>;
+// TM: rows per lane (tile_m by default).
+template <typename R, int TM = tile_m<R>()> struct TileBuf {
+  using L = SmemLayout<R, TM>;
   static constexpr int ELEMS = 4 * L::BUF;
-  __device__ static __forceinline__ int slot(int e) { return (e / tile_m<R>()) * L::ROW + e % tile_m<R>(); }
+  __device__ static __forceinline__ int slot(int e) { return (e / TM) * L::ROW + e % TM; }
 };
 
 // Copies rows [0, nt) of the tile starting at element `base` of a, b, c, d
@@ -145,11 +146,12 @@ template <typename R> struct TileBuf {
 // the tile's start is 16-byte aligned (each unit lies inside one lane's
 // chunk row, whose padded start is 16-byte aligned), element-sized copies
 // otherwise (32 consecutive elements per instruction) and for the tail.
-template <typename R>
+template <typename R, int TM = tile_m<R>()>
 __device__ __forceinline__ void stage_tile_rows(const R *a, const R *b, const R *c, const R *d,
                                                 bool vec16, long long base, int nt, R *buf,
                                                 int lane) {
-  using L = SmemLayout<R, tile_m<R>()>;
+  using L = SmemLayout<R, TM>;
+  using TB = TileBuf<R, TM>;
   constexpr int V = 16 / (int)sizeof(R);
   int e0 = 0;
   if (vec16 && base % V == 0) {
@@ -157,7 +159,7 @@ __device__ __forceinline__ void stage_tile_rows(const R *a, const R *b, const R 
 #pragma unroll 4
     for (int u = lane; u < nfull; u += 32) {
       const int e = u * V;
-      const int o = TileBuf<R>::slot(e);
+      const int o = TB::slot(e);
       cp_async16(buf + 0 * L::BUF + o, a + base + e, 16);
       cp_async16(buf + 1 * L::BUF + o, b + base + e, 16);
       cp_async16(buf + 2 * L::BUF + o, c + base + e, 16);
@@ -166,8 +168,8 @@ __device__ __forceinline__ void stage_tile_rows(const R *a, const R *b, const R 
     e0 = nfull * V;
   }
 #pragma unroll 4
-  for (int e = e0 + lane; e < tile_rows<R>(); e += 32) {
-    const int o = TileBuf<R>::slot(e);
+  for (int e = e0 + lane; e < 32 * TM; e += 32) {
+    const int o = TB::slot(e);
     if (e < nt) {
       cp_async_elem<R>(buf + 0 * L::BUF + o, a + base + e);
       cp_async_elem<R>(buf + 1 * L::BUF + o, b + base + e);
