@@ -41,7 +41,11 @@ def _field(shape, dtype, seed=0):
 
 @pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 1e-5)])
 @pytest.mark.parametrize("shape", [(16, 18, 20), (9, 33, 64), (40, 6, 7), (3, 5, 600),
-                                   (70, 3, 2), (24, 300, 20), (300, 12, 16)])
+                                   (70, 3, 2), (24, 300, 20), (300, 12, 16),
+                                   # y and z systems of 65-512 rows over x extents of
+                                   # whole 128-byte groups (every chunk shape of the
+                                   # streaming solves, Inc included)
+                                   (130, 40, 64), (12, 257, 192), (300, 70, 128)])
 @pytest.mark.parametrize("alpha", [1.0, 0.5])
 @pytest.mark.parametrize("arrays", [False, True], ids=["fused", "arrays"])
 def test_native_step_against_oracle(shape, dtype, tol, alpha, arrays, oracle):
@@ -59,7 +63,7 @@ def test_native_step_against_oracle(shape, dtype, tol, alpha, arrays, oracle):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-@pytest.mark.parametrize("shape", [(130, 200, 160), (72, 100, 300)])
+@pytest.mark.parametrize("shape", [(130, 200, 160), (72, 100, 300), (72, 300, 256)])
 def test_fused_equals_arrays(shape, dtype):
     """Where both forms pick the same chunking (x: 129..512 rows, y and z:
     65..512 rows) the fused timestep runs the array timestep's right-hand-side
