@@ -113,6 +113,11 @@ def _solve_split(dims, sd, splits, dtype, inc, seed):
     ([33, 3, 2], 0, [2, 29, 2]),
     ([256, 8, 8], 0, [128, 128]),
     ([16, 16, 300], 2, [100, 150, 50]),
+    # x segments of 32 M rows: the warp-tile reduction (M = 8, 16), beside
+    # one that takes the lane-per-system reduction (64 rows)
+    ([512, 6, 5], 0, [256, 256]),
+    ([1024, 3, 4], 0, [512, 512]),
+    ([320, 4, 3], 0, [256, 64]),
 ])
 def test_distributed_f64(dims, sd, splits, oracle):
     (a, b, c, d0), x, _ = _solve_split(dims, sd, splits, np.float64, False, seed=sum(splits))
@@ -121,7 +126,9 @@ def test_distributed_f64(dims, sd, splits, oracle):
     assert normwise(x, ref) <= 1e-12
 
 
-@pytest.mark.parametrize("dims,sd,splits", [([16, 24, 10], 1, [8, 16]), ([6, 5, 90], 2, [30, 30, 30])])
+@pytest.mark.parametrize("dims,sd,splits", [([16, 24, 10], 1, [8, 16]), ([6, 5, 90], 2, [30, 30, 30]),
+                                            ([512, 4, 3], 0, [128, 256, 128]),
+                                            ([2048, 3, 2], 0, [1024, 1024])])
 def test_distributed_f32(dims, sd, splits, oracle):
     (a, b, c, d0), x, _ = _solve_split(dims, sd, splits, np.float32, False, seed=3)
     ref = d0.astype(np.float64)
@@ -136,6 +143,16 @@ def test_distributed_inc_leaves_d(sd, oracle):
     (a, b, c, d0), d_after, u = _solve_split(dims, sd, splits, np.float64, True, seed=11)
     ref = d0.copy()
     oracle.strided_batch(a, b, c, ref, dims, sd)
+    assert normwise(u, ref) <= 1e-12
+    assert np.array_equal(d_after, d0)
+
+
+def test_distributed_inc_tile_segments(oracle):
+    """Inc through the warp-tile reduction (x segments of 256 rows)."""
+    dims = [512, 5, 4]
+    (a, b, c, d0), d_after, u = _solve_split(dims, 0, [256, 256], np.float64, True, seed=13)
+    ref = d0.copy()
+    oracle.strided_batch(a, b, c, ref, dims, 0)
     assert normwise(u, ref) <= 1e-12
     assert np.array_equal(d_after, d0)
 

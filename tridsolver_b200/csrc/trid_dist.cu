@@ -4,9 +4,11 @@
 // (scalar/src/cuda/trid_cuda_mpi.cu:609-755 with the ALLGATHER strategy,
 // :218-330; forward pass scalar/src/cuda/trid_linear_mpi.hpp:49-100):
 //
-//  1. reduce: one thread per system sweeps its segment once and leaves two
-//     rows with unit diagonals that couple the segment's first and last
-//     unknowns to the neighbouring ranks' boundary unknowns,
+//  1. reduce: one thread per system sweeps its segment once (or, for
+//     contiguous segments of 32 M rows, a warp reduces the segment as one
+//     tile of the tiled long path) and leaves two rows with unit diagonals
+//     that couple the segment's first and last unknowns to the neighbouring
+//     ranks' boundary unknowns,
 //         top:    A0 x_prev + x_0     + C0 x_{n-1} = D0
 //         bottom: A1 x_0    + x_{n-1} + C1 x_next  = D1;
 //     the bottom row is the last row of the forward (Thomas) elimination;
@@ -33,10 +35,13 @@
 // them again).
 #include <cuda_runtime.h>
 
+#include <stdint.h>
+
 #include <mutex>
 #include <set>
 
 #include "trid_internal.h"
+#include "trid_tile.cuh"
 
 namespace trid {
 
@@ -225,6 +230,88 @@ __global__ void __launch_bounds__(128) dist_reduce_contig_kernel(const BatchArgs
   report_bad_pivot(bad, p.flag);
 }
 
+// Segment reduction for contiguous segments of exactly 32 TM rows: a warp
+// per system, the warp-tile reduction of the tiled long path (coalesced
+// staging, chunk elimination, the warp's reduced solve for the segment's own
+// right-hand side and the unit couplings to x_prev and x_next); the
+// segment's first and last unknowns, f = pf + af x_prev + bf x_next and
+// l = pl + al x_prev + bl x_next, give the two rows above
+// (second_level_rows with neither end a system end). Unlike the tiles of one
+// system, a segment keeps its a_0 and c_{n-1}: they are its couplings.
+template <typename R, int TM>
+__global__ void __launch_bounds__(128) dist_reduce_tile_kernel(const BatchArgs<R> p, R *__restrict__ out) {
+  using L = SmemLayout<R, TM>;
+  using TB = TileBuf<R, TM>;
+  extern __shared__ __align__(16) unsigned char dist_smem[];
+  R *buf = reinterpret_cast<R *>(dist_smem) + (threadIdx.x >> 5) * TB::ELEMS;
+  const int lane = threadIdx.x & 31;
+  const long long nsys = p.nsys;
+  auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+  const bool vec16 = al(p.a) && al(p.b) && al(p.c) && al(p.d_in);
+  bool bad = false;
+  for (long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nsys;
+       s += ((long long)gridDim.x * blockDim.x) >> 5) {
+    stage_tile_rows<R, TM>(p.a, p.b, p.c, p.d_in, vec16, sys_base(p, s), 32 * TM, buf, lane);
+    R a[TM], c[TM], d[TM];
+    lds_row<R, TM>(buf + 0 * L::BUF + lane * L::ROW, a);
+    lds_row<R, TM>(buf + 2 * L::BUF + lane * L::ROW, c);
+    lds_row<R, TM>(buf + 3 * L::BUF + lane * L::ROW, d);
+    chunk_forward_staged<R, TM>(a, buf + 1 * L::BUF + lane * L::ROW, c, d, bad);
+    chunk_backward<R, TM, true>(a, c, d, bad);
+    const Row<R> top{a[0], c[0], d[0]}, bot{a[TM - 1], c[TM - 1], d[TM - 1]};
+    R y[3], z[3];
+    reduced_solve3<R>(top, bot, lane == 0 ? -top.A : R(0), lane == 31 ? -bot.C : R(0), lane, y, z, bad);
+    const R pf = shfl_idx(y[0], 0, 32), af = shfl_idx(y[1], 0, 32), bf = shfl_idx(y[2], 0, 32);
+    const R pl = shfl_idx(z[0], 31, 32), al2 = shfl_idx(z[1], 31, 32), bl = shfl_idx(z[2], 31, 32);
+    if (lane == 0) {
+      Row<R> t2, b2;
+      second_level_rows<R>(pf, af, bf, pl, al2, bl, false, false, t2, b2);
+      out[0 * nsys + s] = t2.A;
+      out[1 * nsys + s] = t2.C;
+      out[2 * nsys + s] = t2.D;
+      out[3 * nsys + s] = b2.A;
+      out[4 * nsys + s] = b2.C;
+      out[5 * nsys + s] = b2.D;
+    }
+    __syncwarp();  // the buffer is free for the next system
+  }
+  report_bad_pivot(bad, p.flag);
+}
+
+template <typename R, int TM>
+static cudaError_t launch_dist_reduce_tile(const BatchArgs<R> &p, R *out, cudaStream_t st) {
+  const size_t smem = (size_t)4 * TileBuf<R, TM>::ELEMS * sizeof(R);  // 4 warps
+  auto kern = dist_reduce_tile_kernel<R, TM>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const long long need = (p.nsys + 3) / 4;
+  const long long cap = (long long)sms * per_sm;
+  kern<<<(unsigned)(need < cap ? need : cap), 128, smem, st>>>(p, out);
+  return cudaGetLastError();
+}
+
+// The warp-tile reduction where a contiguous segment fills a tile exactly
+// (32 TM rows, TM = 4 .. 16 FP64, 4 .. 32 FP32); cudaErrorNotSupported
+// otherwise.
+template <typename R>
+static cudaError_t launch_dist_reduce_tiles(const BatchArgs<R> &p, R *out, cudaStream_t st) {
+  if (p.stride != 1) return cudaErrorNotSupported;
+  switch (p.N) {
+    case 128: return launch_dist_reduce_tile<R, 4>(p, out, st);
+    case 256: return launch_dist_reduce_tile<R, 8>(p, out, st);
+    case 512: return launch_dist_reduce_tile<R, 16>(p, out, st);
+    case 1024:
+      if constexpr (sizeof(R) == 4) return launch_dist_reduce_tile<R, 32>(p, out, st);
+      return cudaErrorNotSupported;
+    default: return cudaErrorNotSupported;
+  }
+}
+
 // Reduced solve of system s over all ranks' rows and the right-hand-side
 // correction of this rank's segment. g: P blocks of 6 * nsys values (the
 // gathered outputs of dist_reduce_kernel, rank-major); row i of the reduced
@@ -359,15 +446,18 @@ tridStatus_t dist_solve(const tridDistParams *dp, const BatchArgs<R> &p0, int so
   R *send = scratch;
   R *recv = scratch + 6 * p.nsys;
   R *save = recv + (size_t)6 * p.nsys * P;
-  if (p.stride == 1) {
-    long long blocks = (p.nsys + 127) / 128;
-    if (blocks > 148LL * 16) blocks = 148LL * 16;
-    dist_reduce_contig_kernel<R><<<(unsigned)(blocks < 1 ? 1 : blocks), 128, 0, st>>>(p, send);
-  } else {
-    dist_reduce_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, send);
+  e = launch_dist_reduce_tiles<R>(p, send, st);
+  if (e == cudaErrorNotSupported) {
+    if (p.stride == 1) {
+      long long blocks = (p.nsys + 127) / 128;
+      if (blocks > 148LL * 16) blocks = 148LL * 16;
+      dist_reduce_contig_kernel<R><<<(unsigned)(blocks < 1 ? 1 : blocks), 128, 0, st>>>(p, send);
+    } else {
+      dist_reduce_kernel<R><<<grid_for(p.nsys), 128, 0, st>>>(p, send);
+    }
+    e = cudaGetLastError();
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  e = cudaGetLastError();
   tridStatus_t status = TRID_STATUS_SUCCESS;
   if (e == cudaSuccess) {
     const int rc = dp->allgather(send, recv, per_rank, dp->user, st);
