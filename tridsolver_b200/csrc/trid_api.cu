@@ -172,6 +172,16 @@ tridStatus_t make_batch(const R *a, const R *b, const R *c, R *d, R *u, bool inc
     p.st1 = pads[0];
     p.stride = s01;
   }
+  // Systems equally spaced over both enumerating dimensions (no padding
+  // between them, e.g. a z solve with pads[0] == dims[0]) are one flat
+  // dimension when the fastest one is narrower than a 256-byte group:
+  // groups of neighbouring systems then span its rows (8 x 8 x 2^20 FP64
+  // along z: 1.48 -> 1.04 ms). Wider rows keep the two dimensions (32 x 32
+  // x 65536 along z measured 6% slower flat).
+  if (p.st1 == p.n0 * p.st0 && p.n0 * (long long)sizeof(R) < 256) {
+    p.n0 = p.nsys;
+    p.st1 = p.nsys * p.st0;
+  }
   *out = p;
   return TRID_STATUS_SUCCESS;
 }
