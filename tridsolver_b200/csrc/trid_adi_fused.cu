@@ -405,7 +405,7 @@ template <typename R, int T> constexpr int adi_bs() { return T * adi_w<R>(); }
 // are free of bank conflicts).
 //
 // Work: the (tile, plane) steps, tile-major, are split evenly over the grid
-// (one CTA per SM); a CTA whose range crosses into the next tile restarts
+// (the CTAs resident at once); a CTA whose range crosses into the next tile restarts
 // its ring there.
 // TRANS: the transposed solve of the step's x matrix in place (u == du):
 // the right-hand side is the line itself with rows 0 and nx - 1 taken as 0,
@@ -871,15 +871,14 @@ static cudaError_t launch_adi_x_j(const R *u, R *du, const ConstCoef<R> &k, unsi
   return cudaGetLastError();
 }
 
-// Tile of 16 lines with slabs one plane ahead where it fits in shared
-// memory, else 8 lines.
+// Tiles of 8 lines with slabs one plane ahead: two 4-warp CTAs share an SM
+// (ms per step, 256^3 FP64 / 512x512x128 FP32: 0.191 / 0.224 against 0.196
+// / 0.228 with 16 lines at one CTA per SM; 16 lines two planes ahead 0.197,
+// 8 lines two planes ahead 0.228 / 0.257, 4 lines 0.208 FP64).
 template <typename R, int M, bool VEC, bool TRANS = false>
 static cudaError_t launch_adi_x_mv(const R *u, R *du, const ConstCoef<R> &k, unsigned *flag, int nx,
                                    int ny, int nz, cudaStream_t st) {
-  if constexpr (adi_x_smem<R, M, VEC, 16, 1>() <= 224 * 1024)
-    return launch_adi_x_j<R, M, VEC, 16, 1, TRANS>(u, du, k, flag, nx, ny, nz, st);
-  else
-    return launch_adi_x_j<R, M, VEC, 8, 1, TRANS>(u, du, k, flag, nx, ny, nz, st);
+  return launch_adi_x_j<R, M, VEC, 8, 1, TRANS>(u, du, k, flag, nx, ny, nz, st);
 }
 
 template <typename R>
