@@ -124,6 +124,23 @@ EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *
 EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a, const float *b,
                                            const float *c, float *d, const int64_t *offsets,
                                            long long nsys);
+/* As above, with the batch's element count given by the caller: nelems >=
+ * offsets[nsys] - offsets[0] (a larger count only sizes more scratch). The
+ * call above reads those two offsets back to size its scratch, a
+ * synchronisation; this one reads nothing back, so with blocking off it
+ * only enqueues work and can be captured into a CUDA graph (its scratch
+ * then comes from the graph's own allocation). A count below the batch's is
+ * refused on the device before anything is written: d is left as it was
+ * and a blocking call returns TRID_STATUS_INVALID_VALUE (a non-blocking
+ * call cannot report it). nelems < 0 returns TRID_STATUS_INVALID_VALUE. */
+EXTERN_C tridStatus_t tridDmtsvRaggedBatchSized(const TridParams *ctx, const double *a,
+                                                const double *b, const double *c, double *d,
+                                                const int64_t *offsets, long long nsys,
+                                                long long nelems);
+EXTERN_C tridStatus_t tridSmtsvRaggedBatchSized(const TridParams *ctx, const float *a,
+                                                const float *b, const float *c, float *d,
+                                                const int64_t *offsets, long long nsys,
+                                                long long nelems);
 /* Times, per length class up to one warp's worth of rows, every
  * rows-per-lane choice of a warp per system and the staged tile path, on
  * this device (uniform synthetic batches, about a second), and keeps the

@@ -245,3 +245,12 @@ def test_no_alloc_entry_refuses_a_distributed_ctx():
         st = fn(ctypes.addressof(dc.ctx), ptr, ptr, ptr, ptr, 2, 1, dims, dims)
     assert st == TridStatus.INVALID_VALUE
     assert not buf.any()
+
+
+def test_sized_ragged_call_checks_its_count_without_device():
+    """The sized ragged entry points refuse a negative element count, and an
+    empty batch succeeds, before any device is touched."""
+    for fn in (tb.tridDmtsvRaggedBatchSized, tb.tridSmtsvRaggedBatchSized):
+        assert fn(None, None, None, None, None, None, 0, -1) == TridStatus.INVALID_VALUE
+        assert fn(None, None, None, None, None, None, 0, 0) == TridStatus.SUCCESS
+        assert fn(None, None, None, None, None, None, -3, 0) == TridStatus.INVALID_VALUE

@@ -141,6 +141,94 @@ def test_bounded_wait_runs_out_and_is_reported(oracle):
         assert np.max(np.abs(got.astype(np.float64) - want)) / np.max(np.abs(want)) <= tol
 
 
+def _sized(dt):
+    return tb.tridDmtsvRaggedBatchSized if dt == np.float64 else tb.tridSmtsvRaggedBatchSized
+
+
+@pytest.mark.parametrize("dt,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_sized_call_matches_the_counted_one(dt, tol, oracle):
+    """tridDmtsvRaggedBatchSized with the exact element count, and with a
+    larger one, gives the counted call's result bit for bit (the same
+    kernels; only the scratch sizing differs), and the oracle's."""
+    lengths = np.array(EDGE * 2)
+    np.random.default_rng(9).shuffle(lengths)
+    arrs, offs = _batch(lengths, dt, seed=10)
+    st, first = _run(arrs, offs, dt)
+    assert st == 0
+    for nelems in (int(offs[-1]), int(offs[-1]) + 12345):
+        ta, tb_, tc, td = (torch.from_numpy(v).cuda() for v in arrs)
+        st = _sized(dt)(None, ta, tb_, tc, td, torch.from_numpy(offs).cuda(), len(lengths), nelems)
+        torch.cuda.synchronize()
+        assert st == 0
+        assert np.array_equal(td.cpu().numpy(), first)
+    want = arrs[3].copy()
+    oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
+    assert np.max(np.abs(first.astype(np.float64) - want)) / np.max(np.abs(want)) <= tol
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_sized_call_refuses_a_short_count(dt):
+    """A count below offsets[nsys] - offsets[0] is refused on the device
+    before anything is written: d keeps its values, the blocking call returns
+    INVALID_VALUE, and a negative count is refused on the host."""
+    lengths = np.array([3000, 40, 9000, 700, 2048, 5] * 8)
+    arrs, offs = _batch(lengths, dt, seed=11)
+    total = int(offs[-1])
+    to = torch.from_numpy(offs).cuda()
+    for nelems in (total - 1, total // 4, 0):
+        ta, tb_, tc, td = (torch.from_numpy(v).cuda() for v in arrs)
+        st = _sized(dt)(None, ta, tb_, tc, td, to, len(lengths), nelems)
+        torch.cuda.synchronize()
+        assert st == tb.TridStatus.INVALID_VALUE, nelems
+        assert np.array_equal(td.cpu().numpy(), arrs[3])
+    st = _sized(dt)(None, ta, tb_, tc, td, to, len(lengths), -1)
+    assert st == tb.TridStatus.INVALID_VALUE
+
+
+@pytest.mark.parametrize("dt,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_sized_call_replays_in_a_cuda_graph(dt, tol, oracle):
+    """The sized call, non-blocking, captured into a CUDA graph after one
+    eager call: each replay copies the current right-hand side into d and
+    solves it (the scratch is the graph's own allocation), and matches the
+    oracle for three different right-hand sides."""
+    lengths = np.array([1, 31, 33, 200, 513, 1025, 3000, 9000, 16384, 64] * 6)
+    arrs, offs = _batch(lengths, dt, seed=12)
+    ta, tb_, tc, td = (torch.from_numpy(v).cuda() for v in arrs)
+    rhs = td.clone()
+    to = torch.from_numpy(offs).cuda()
+    nelems = int(offs[-1])
+
+    def launch():
+        td.copy_(rhs)
+        st = _sized(dt)(None, ta, tb_, tc, td, to, len(lengths), nelems)
+        assert st == 0
+
+    with tb.on_stream(blocking=False):
+        launch()
+    torch.cuda.synchronize()
+    tb.pivot_status()  # clears the record
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            with tb.on_stream(s, blocking=False):
+                launch()
+    torch.cuda.current_stream().wait_stream(s)
+    rng = np.random.default_rng(13)
+    for rep in range(3):
+        d0 = rng.standard_normal(nelems).astype(dt)
+        rhs.copy_(torch.from_numpy(d0))
+        g.replay()
+        torch.cuda.synchronize()
+        want = d0.copy()
+        oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
+        got = td.cpu().numpy().astype(np.float64)
+        assert np.max(np.abs(got - want)) / np.max(np.abs(want)) <= tol, rep
+    assert tb.pivot_status() == tb.TridStatus.SUCCESS
+    del g
+
+
 @pytest.mark.parametrize("dt,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
 def test_bench_batch_of_200000_systems(dt, tol, oracle):
     """The benchmark's ragged batch itself: 200,000 systems with lengths

@@ -8,6 +8,7 @@ entry points, include/tridsolver.h). This package binds it for Python.
 from .api import (  # noqa: F401
     FAMILY_AUTO, FAMILY_HYBRID, FAMILY_LONG, FAMILY_PCR, TridError, TridParams, TridStatus,
     autotune, autotune_reset, describe_plan, ragged_autotune, ragged_table, tridDmtsvRaggedBatch, tridSmtsvRaggedBatch,
+    tridDmtsvRaggedBatchSized, tridSmtsvRaggedBatchSized,
     force_plan, force_stream, force_tma, force_systems_per_block, get_blocking, launch_count, on_stream, pivot_status,
     release_scratch, set_tracing,
     set_mixed_mode,

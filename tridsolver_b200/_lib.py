@@ -44,6 +44,8 @@ SYMBOLS = {
     "tridDescribePlanInc": (_I, [_I, _I, _I, _IP, _IP, _I, ctypes.c_char_p, _I]),
     "tridDmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
     "tridSmtsvRaggedBatch": (_I, [_P] * 6 + [ctypes.c_longlong]),
+    "tridDmtsvRaggedBatchSized": (_I, [_P] * 6 + [ctypes.c_longlong] * 2),
+    "tridSmtsvRaggedBatchSized": (_I, [_P] * 6 + [ctypes.c_longlong] * 2),
     "tridRaggedAutotune": (_I, [_I]),
     "tridRaggedTable": (_I, [_I, _IP, _I]),
     "tridRaggedSetWaitBound": (_I, [ctypes.c_ulonglong, _I]),

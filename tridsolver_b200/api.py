@@ -170,6 +170,19 @@ def tridSmtsvRaggedBatch(ctx, a, b, c, d, offsets, nsys):
                                             _addr(offsets), int(nsys))
 
 
+def tridDmtsvRaggedBatchSized(ctx, a, b, c, d, offsets, nsys, nelems):
+    """Ragged batch with the element count given (nelems >= offsets[nsys] -
+    offsets[0]): nothing is read back, so the call can be captured into a
+    CUDA graph with blocking off. Returns the status code."""
+    return _lib.load().tridDmtsvRaggedBatchSized(_ctx(ctx), _addr(a), _addr(b), _addr(c),
+                                                 _addr(d), _addr(offsets), int(nsys), int(nelems))
+
+
+def tridSmtsvRaggedBatchSized(ctx, a, b, c, d, offsets, nsys, nelems):
+    return _lib.load().tridSmtsvRaggedBatchSized(_ctx(ctx), _addr(a), _addr(b), _addr(c),
+                                                 _addr(d), _addr(offsets), int(nsys), int(nelems))
+
+
 def ragged_autotune(dtype_bytes):
     st = _lib.load().tridRaggedAutotune(int(dtype_bytes))
     if st != 0:

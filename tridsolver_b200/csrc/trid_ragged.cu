@@ -88,6 +88,7 @@ template <typename R> struct RaggedArgs {
   unsigned *error;                  // 1: a system longer than 16384 rows; 2: a wait gave up;
                                     // 3: the tile table was too small
   long long max_tiles;              // entries of tile_meta / tile_base / tile_rows / tile_fl
+  long long nelems;                 // element count the caller gave (-1: read back)
   bool vec16;                       // a, b, c, d all 16-byte aligned
   unsigned wait_limit;              // polls before a wait gives up (kWaitLimit by default)
   bool withhold;                    // failure-detection tests: never publish (waits run out)
@@ -115,6 +116,9 @@ __device__ __forceinline__ int length_class(long long n) {
 
 template <typename R>
 __global__ void ragged_hist_kernel(RaggedArgs<R> p, unsigned *hist, unsigned long long *tiles) {
+  // a caller's count below the batch's: refused before anything is written
+  if (p.nelems >= 0 && blockIdx.x == 0 && threadIdx.x == 0 && p.off[p.nsys] - p.off[0] > p.nelems)
+    atomicExch(p.error, 3u);
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < p.nsys;
        s += (long long)gridDim.x * blockDim.x) {
     const long long n = p.off[s + 1] - p.off[s];
@@ -629,21 +633,29 @@ static std::atomic<unsigned long long> g_wait_polls{0};
 static std::atomic<int> g_withhold{0};
 
 template <typename R>
-static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t st) {
+static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, long long elems,
+                                 cudaStream_t st) {
   for (int c = 0; c < kClasses; ++c) p.mtab[c] = mtab[c];
   // classes beyond one warp are always tile classes
   for (int c = 0; c < kClasses; ++c)
     if ((1LL << c) > ragged_warp_max<R>()) p.mtab[c] = 0;
-  // the tile scratch is sized by the batch's element count: two offsets
-  // are read back (a short synchronisation on `st`)
-  int64_t ends[2] = {0, 0};
-  cudaError_t e = cudaMemcpyAsync(&ends[0], p.off, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&ends[1], p.off + p.nsys, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return e;
-  const long long elems = ends[1] - ends[0];
-  if (elems < 0) return cudaErrorInvalidValue;
+  // The tile scratch is sized by the batch's element count. Without a
+  // count from the caller (elems < 0) two offsets are read back, a short
+  // synchronisation on `st`; with one, nothing is read back and the call
+  // can be captured. The order kernel refuses a tile table the count
+  // undersizes (error 3) and the solve then writes nothing.
+  cudaError_t e = cudaSuccess;
+  const long long given = elems;
+  if (elems < 0) {
+    int64_t ends[2] = {0, 0};
+    e = cudaMemcpyAsync(&ends[0], p.off, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ends[1], p.off + p.nsys, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    elems = ends[1] - ends[0];
+    if (elems < 0) return cudaErrorInvalidValue;
+  }
   const long long max_tiles = elems / rtile_rows<R>() + p.nsys + 1;
   // scratch: header | order (int, nsys) | done, ready (u32, nsys each) |
   // tile_meta (int4, max_tiles) | tile_base (i64) | tile_rows (6 R) | tile_fl (2 R)
@@ -689,6 +701,7 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
   p.sys_done = done;
   p.sys_ready = ready;
   p.max_tiles = max_tiles;
+  p.nelems = given;
   p.counter = counter;
   p.error = error;
   {
@@ -736,7 +749,7 @@ static cudaError_t launch_ragged(RaggedArgs<R> p, const int *mtab, cudaStream_t 
 
 template <typename R>
 static tridStatus_t ragged(const R *a, const R *b, const R *c, R *d, const int64_t *offsets,
-                           long long nsys) {
+                           long long nsys, long long nelems) {
   if (nsys < 0) return TRID_STATUS_INVALID_VALUE;
   if (nsys == 0) return TRID_STATUS_SUCCESS;
   if (!a || !b || !c || !d || !offsets || nsys > 0x7fffffffLL) return TRID_STATUS_INVALID_VALUE;
@@ -761,7 +774,7 @@ static tridStatus_t ragged(const R *a, const R *b, const R *c, R *d, const int64
   p.nsys = nsys;
   p.flag = pivot_flag_device();
   if (cfg.blocking) pivot_flag_take();
-  cudaError_t e = launch_ragged<R>(p, mt, cfg.stream);
+  cudaError_t e = launch_ragged<R>(p, mt, nelems, cfg.stream);
   if (e == cudaErrorNotSupported) return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED;
   if (e == cudaErrorInvalidValue) return TRID_STATUS_INVALID_VALUE;
   if (e != cudaSuccess) return status_of(e);
@@ -837,7 +850,7 @@ static tridStatus_t autotune(int dev) {
       float ms = 1e30f;
       for (int rep = 0; rep < 3; ++rep) {
         cudaEventRecord(e0, st);
-        cudaError_t e = launch_ragged<R>(p, trial, st);
+        cudaError_t e = launch_ragged<R>(p, trial, nsys * len, st);
         cudaEventRecord(e1, st);
         if (e != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
           status = TRID_STATUS_EXECUTION_FAILED;
@@ -874,7 +887,7 @@ EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *
                                            long long nsys) {
   const TraceScope trace("tridDmtsvRaggedBatch");
   (void)ctx;
-  return ragged<double>(a, b, c, d, offsets, nsys);
+  return ragged<double>(a, b, c, d, offsets, nsys, -1);
 }
 
 EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a, const float *b,
@@ -882,7 +895,27 @@ EXTERN_C tridStatus_t tridSmtsvRaggedBatch(const TridParams *ctx, const float *a
                                            long long nsys) {
   const TraceScope trace("tridSmtsvRaggedBatch");
   (void)ctx;
-  return ragged<float>(a, b, c, d, offsets, nsys);
+  return ragged<float>(a, b, c, d, offsets, nsys, -1);
+}
+
+EXTERN_C tridStatus_t tridDmtsvRaggedBatchSized(const TridParams *ctx, const double *a,
+                                                const double *b, const double *c, double *d,
+                                                const int64_t *offsets, long long nsys,
+                                                long long nelems) {
+  const TraceScope trace("tridDmtsvRaggedBatchSized");
+  (void)ctx;
+  if (nelems < 0) return TRID_STATUS_INVALID_VALUE;
+  return ragged<double>(a, b, c, d, offsets, nsys, nelems);
+}
+
+EXTERN_C tridStatus_t tridSmtsvRaggedBatchSized(const TridParams *ctx, const float *a,
+                                                const float *b, const float *c, float *d,
+                                                const int64_t *offsets, long long nsys,
+                                                long long nelems) {
+  const TraceScope trace("tridSmtsvRaggedBatchSized");
+  (void)ctx;
+  if (nelems < 0) return TRID_STATUS_INVALID_VALUE;
+  return ragged<float>(a, b, c, d, offsets, nsys, nelems);
 }
 
 EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes) {
