@@ -114,10 +114,9 @@ EXTERN_C tridStatus_t tridForceStream(int mode);
  * persistent launch of independent warps: short systems (up to 256 rows)
  * one per warp with a per-length-class rows-per-lane table (pure PCR up to
  * 32 rows, the partition hybrid beyond), longer ones cut into tiles of 512
- * rows (double) / 1024 rows (float), one warp per tile, joined by a
- * second-level system of two rows per tile (up to 16384 rows per system; a
- * longer system makes a blocking call return
- * TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
+ * rows, one warp per tile, joined by a second-level system of two rows per
+ * tile (up to 16384 rows per system; a longer system makes a blocking call
+ * return TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED). */
 EXTERN_C tridStatus_t tridDmtsvRaggedBatch(const TridParams *ctx, const double *a, const double *b,
                                            const double *c, double *d, const int64_t *offsets,
                                            long long nsys);
@@ -145,8 +144,7 @@ EXTERN_C tridStatus_t tridSmtsvRaggedBatchSized(const TridParams *ctx, const flo
  * rows-per-lane choice of a warp per system and the staged tile path, on
  * this device (uniform synthetic batches, about a second), and keeps the
  * fastest for later ragged calls of that precision on the current device.
- * Longer systems always take tiles (512 rows double / 1024 rows float,
- * N <= 16384). */
+ * Longer systems always take tiles (512 rows, N <= 16384). */
 EXTERN_C tridStatus_t tridRaggedAutotune(int dtype_bytes);
 /* Failure-detection hook (process-wide; tests only). A warp holding one tile
  * of a multi-tile system waits, bounded, for the warp that solves the

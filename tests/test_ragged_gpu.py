@@ -4,10 +4,10 @@ Each system is checked against the oracle's per-system Thomas solve
 (oracle_ragged_*, the reference's trid_scalar, scalar/src/cpu/
 trid_cpu.cpp:312-353): normwise <= 1e-12 (FP64) / 1e-5 (FP32), per system
 and over the batch. Lengths cover every path: empty and one-row systems,
-pure PCR (<= 32), the warp hybrid for short classes, single tiles (512 rows
-FP64, 1024 rows FP32) and systems of 2 to 32 (FP32: 16) tiles coupled
-through the second-level solve (tile boundaries at every offset), up to the
-16384-row limit, in shuffled order.
+pure PCR (<= 32), the warp hybrid for short classes, single tiles (512
+rows) and systems of 2 to 32 tiles coupled through the second-level solve
+(tile boundaries at every offset), up to the 16384-row limit, in shuffled
+order.
 """
 
 import numpy as np
@@ -261,3 +261,4 @@ def test_bench_batch_of_200000_systems(dt, tol, oracle):
     smax = np.maximum.reduceat(np.abs(want), offs[:-1])
     dmax = np.maximum.reduceat(diff, offs[:-1])
     assert np.max(dmax / smax) <= 10 * tol
+
