@@ -1,4 +1,4 @@
-"""GPU: the full BASELINE grids, elementwise, against the reference library.
+"""GPU: the full benchmark grids, elementwise, against the reference library.
 
 Every case of the drop-in sweep: 256^3 and 512^3 grids, FP64 and FP32,
 solvedim 0, 1 and 2, overwrite and Inc, with the benchmark's inputs

@@ -7,7 +7,7 @@
   CPU library: normwise relative error <= 1e-12 (FP64) / 1e-5 (FP32);
 * every kernel family (hybrid for each rows-per-thread, pure PCR, the long
   multi-block path) forced on the same problems;
-* the full BASELINE grids (256^3, 512^3 FP64) through size-independent
+* the full benchmark grids (256^3, 512^3 FP64) through size-independent
   checks: the residual of T x = d, and sampled systems against the oracle.
 """
 
