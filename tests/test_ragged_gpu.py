@@ -262,3 +262,25 @@ def test_bench_batch_of_200000_systems(dt, tol, oracle):
     dmax = np.maximum.reduceat(diff, offs[:-1])
     assert np.max(dmax / smax) <= 10 * tol
 
+
+
+@pytest.mark.parametrize("dt,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+@pytest.mark.parametrize("lead", [1, 2, 3, 5])
+def test_systems_at_every_alignment(dt, tol, lead, oracle):
+    """Systems starting at every element offset modulo 16 bytes (the lead
+    system's length shifts the rest), with lengths at and around tile
+    multiples up to the 16384-row limit: tiles that start on a 16-byte
+    boundary stage in 16-byte units, the others element by element, and
+    every system matches the oracle."""
+    lengths = np.array([lead, 16384, 510, 511, 512, 513, 1022, 1023, 1024, 1025, 16381, 3, 16384,
+                        16383, 700, 1, 2047, 16382])
+    arrs, offs = _batch(lengths, dt, seed=20 + lead)
+    want = arrs[3].copy()
+    oracle.ragged(arrs[0], arrs[1], arrs[2], want, offs)
+    st, got = _run(arrs, offs, dt)
+    assert st == 0
+    for k in range(len(lengths)):
+        s, e = offs[k], offs[k + 1]
+        den = np.max(np.abs(want[s:e]))
+        err = np.max(np.abs(got[s:e].astype(np.float64) - want[s:e])) / den
+        assert err <= tol, (k, e - s, s % 4, err)
